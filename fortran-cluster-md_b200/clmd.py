@@ -1,0 +1,440 @@
+"""Python host mirror of the engine's C ABI (include/clmd.h), over ctypes.
+
+The product is libclmd.so (CUDA, sm_100a) next to this file; this module only
+binds it.  `System` wraps one device-resident system and exposes the
+reference's subroutine surface under the reference's names (neighbor,
+accatom, integrator, thermostat, stopdead, stoddard, chk_nucleation) plus
+the device-resident main loop `run`.  There is no CPU fallback: creating a
+System raises if the library is missing or no GPU is visible.
+
+Reduced-unit configurations (sigma = eps = m = 1, kB*T = T*) are built by
+`lj_config`; the reference's internal Boltzmann constant is kept, so
+att = T* / CIKB.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libclmd.so")
+
+MXSORTS = 10
+MXA = 6000
+CIKB = 1.38066e-6
+CIMU = 1.66056
+
+OK = 0
+ERR_SKIN = 1
+ERR_LIST_OVERFLOW = 2
+ERR_NH_NOCONVERGE = 3
+ERR_BAD_SPECIES = 4
+ERR_ARG = 5
+ERR_CUDA = 6
+ERR_NOMEM = 7
+ERR_NO_DEVICE = 8
+ERR_TIMEOUT = 9
+
+INT_VERLET = 0
+INT_NOSE = 1
+CLU_STILLINGER = 0
+CLU_FRENKEL = 1
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+
+class Config(C.Structure):
+    """clmd_config (include/clmd.h)."""
+
+    _fields_ = [
+        ("apmas", C.c_double * MXSORTS),
+        ("apsig", C.c_double * MXSORTS),
+        ("apeps", C.c_double * MXSORTS),
+        ("att", C.c_double),
+        ("atskin", C.c_double),
+        ("atrcut", C.c_double),
+        ("atrskin", C.c_double),
+        ("Q", C.c_double),
+        ("boxx", C.c_double),
+        ("boxy", C.c_double),
+        ("boxz", C.c_double),
+        ("dt", C.c_double),
+        ("nlist_cap", C.c_int64),
+        ("natom", C.c_int32),
+        ("atsorts", C.c_int32),
+        ("apnum", C.c_int32 * MXSORTS),
+        ("atnenum", C.c_int32),
+        ("nbtim", C.c_int32),
+        ("btim", C.c_int32),
+        ("csover", C.c_int32),
+        ("clwait", C.c_int32),
+        ("ftcsi", C.c_int32),
+        ("integrator", C.c_int32),
+        ("clustering", C.c_int32),
+        ("precision", C.c_int32),
+        ("apth", C.c_char * MXSORTS),
+        ("ethst", C.c_char),
+        ("clnuctrl", C.c_char),
+        ("pad", C.c_char * 4),
+    ]
+
+
+class Scalars(C.Structure):
+    """clmd_scalars (include/clmd.h)."""
+
+    _fields_ = [
+        ("ekin", C.c_double),
+        ("sumv2", C.c_double),
+        ("epot", C.c_double),
+        ("H", C.c_double),
+        ("psi", C.c_double),
+        ("s", C.c_double),
+        ("atrskin", C.c_double),
+        ("dmms", C.c_double),
+        ("dmmsu", C.c_double),
+        ("dmmax", C.c_double),
+        ("dmmav", C.c_double),
+        ("dmmh", C.c_double * 256),
+        ("virial", C.c_double),
+        ("npairs_half", C.c_int64),
+        ("dmmst", C.c_int32),
+        ("dmmi", C.c_int32),
+        ("clbrkt", C.c_int32),
+        ("cnum", C.c_int32),
+        ("cnumf", C.c_int32),
+        ("cstep", C.c_int32),
+        ("cbiggest", C.c_int32),
+        ("cbiggestf", C.c_int32),
+        ("clookfor", C.c_int32),
+        ("clookforf", C.c_int32),
+        ("status", C.c_int32),
+        ("fail_step", C.c_int32),
+        ("nh_iters", C.c_int32),
+        ("nrebuild", C.c_int32),
+        ("last_rebuild_step", C.c_int32),
+        ("aborted", C.c_int32),
+        ("maxcs", C.c_int32),
+        ("pad", C.c_int32),
+    ]
+
+    def as_dict(self):
+        out = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            out[name] = list(v) if name == "dmmh" else v
+        return out
+
+
+_I32P = C.POINTER(C.c_int32)
+_F64P = C.POINTER(C.c_double)
+
+
+class ClusterView(C.Structure):
+    """clmd_cluster_view (include/clmd.h)."""
+
+    _fields_ = [
+        ("cl", _I32P), ("cs", _I32P), ("csi", _I32P),
+        ("cek", _F64P), ("ceks", _F64P),
+        ("clf", _I32P), ("csf", _I32P), ("csif", _I32P),
+        ("cekf", _F64P), ("ceksf", _F64P),
+        ("cgs", _I32P), ("cgsa", _I32P), ("cgsf", _I32P), ("cgsfa", _I32P),
+        ("cfpt", _I32P), ("cfptf", _I32P),
+    ]
+
+
+# (name, dtype, length kind) of every cluster output: "N" or "N1" (= N+1)
+CLUSTER_FIELDS = [
+    ("cl", np.int32, "N"), ("cs", np.int32, "N"), ("csi", np.int32, "N1"),
+    ("cek", np.float64, "N"), ("ceks", np.float64, "N1"),
+    ("clf", np.int32, "N"), ("csf", np.int32, "N1"), ("csif", np.int32, "N1"),
+    ("cekf", np.float64, "N1"), ("ceksf", np.float64, "N1"),
+    ("cgs", np.int32, "N"), ("cgsa", np.int32, "N"), ("cgsf", np.int32, "N1"),
+    ("cgsfa", np.int32, "N1"), ("cfpt", np.int32, "N"), ("cfptf", np.int32, "N"),
+]
+
+
+def ptr(a, ctype):
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Loads libclmd.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(
+            f"libclmd.so not found at {path}: build it with `make -C {HERE}` "
+            "(the engine has no CPU fallback)")
+    lib = C.CDLL(path)
+    P = C.c_void_p
+    d = C.POINTER(C.c_double)
+    i = C.POINTER(C.c_int32)
+    sig = {
+        "clmd_create": ([C.POINTER(Config), C.POINTER(P)], C.c_int),
+        "clmd_destroy": ([P], C.c_int),
+        "clmd_set_state": ([P, d, d, d, d, d, d, d, d, d, i, C.POINTER(Scalars)], C.c_int),
+        "clmd_get_state": ([P, d, d, d, d, d, d, d, d, d, C.POINTER(Scalars)], C.c_int),
+        "clmd_get_scalars": ([P, C.POINTER(Scalars)], C.c_int),
+        "clmd_set_scalars": ([P, C.POINTER(Scalars)], C.c_int),
+        "clmd_clear_status": ([P], C.c_int),
+        "clmd_neighbor": ([P, i], C.c_int),
+        "clmd_accatom": ([P], C.c_int),
+        "clmd_accwall": ([P], C.c_int),
+        "clmd_zero_acc": ([P], C.c_int),
+        "clmd_integrator": ([P, C.c_int32], C.c_int),
+        "clmd_thermostat": ([P, C.c_int32], C.c_int),
+        "clmd_stopdead": ([P, C.c_int32], C.c_int),
+        "clmd_stoddard": ([P, C.c_int32], C.c_int),
+        "clmd_chk_nucleation": ([P, i], C.c_int),
+        "clmd_run": ([P, C.c_int32, C.c_int32, i], C.c_int),
+        "clmd_get_halflist": ([P, i, C.c_int64, i, C.POINTER(C.c_int64)], C.c_int),
+        "clmd_get_clusters": ([P, C.POINTER(ClusterView)], C.c_int),
+        "clmd_synchronize": ([P], C.c_int),
+        "clmd_stream": ([P], C.c_void_p),
+        "clmd_kernel_launches": ([P], C.c_int64),
+        "clmd_init_random": ([C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double,
+                              C.c_double, C.c_uint64, d, d, d, d, d, d], C.c_int),
+        "clmd_status_string": ([C.c_int], C.c_char_p),
+        "clmd_last_status": ([], C.c_int32),
+        "clmd_struct_size": ([C.c_int], C.c_int64),
+        "clmd_scalars_init": ([C.POINTER(Config), C.POINTER(Scalars)], None),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = lib
+    return lib
+
+
+def status_string(code: int) -> str:
+    return load().clmd_status_string(code).decode()
+
+
+class ClmdError(RuntimeError):
+    def __init__(self, code, what=""):
+        self.code = code
+        super().__init__(f"{what}: status {code} ({status_string(code)})")
+
+
+def lj_config(n, rho, temp, *, rc=2.5, rskin=2.8, atskin=1.5, dt=0.005, nbtim=10,
+              integrator=INT_VERLET, clustering=CLU_STILLINGER, ftcsi=100, csover=0,
+              clwait=0, clnuctrl="-", ethst="-", q=None, atnenum=5, btim=0,
+              precision=PREC_FP64, nlist_cap=0, species=None) -> Config:
+    """A reduced-unit LJ configuration (sigma = eps = m = 1) at number density
+    rho and temperature T* in a cubic box; `species` optionally gives a second
+    species as dict(n=..., sigma=..., eps=..., mass=..., thermo='X')."""
+    c = Config()
+    L = (n / rho) ** (1.0 / 3.0)
+    c.boxx = c.boxy = c.boxz = L
+    c.natom = n
+    c.apmas[0] = 1.0
+    c.apsig[0] = 1.0
+    c.apeps[0] = 1.0
+    apth = [b"-"] * MXSORTS
+    if species:
+        n2 = species["n"]
+        c.atsorts = 2
+        c.apnum[0] = n - n2
+        c.apnum[1] = n2
+        c.apmas[1] = species.get("mass", 1.0)
+        c.apsig[1] = species.get("sigma", 1.0)
+        c.apeps[1] = species.get("eps", 1.0)
+        apth[1] = species.get("thermo", "-").encode()
+    else:
+        c.atsorts = 1
+        c.apnum[0] = n
+    c.apth = b"".join(apth)
+    c.att = temp / CIKB
+    c.atskin = atskin
+    c.atrcut = rc
+    c.atrskin = rskin
+    c.dt = dt
+    c.nbtim = nbtim
+    c.btim = btim
+    c.integrator = integrator
+    c.clustering = clustering
+    c.ftcsi = ftcsi
+    c.csover = csover
+    c.clwait = clwait
+    c.clnuctrl = clnuctrl.encode()
+    c.ethst = ethst.encode()
+    c.atnenum = atnenum
+    c.precision = precision
+    c.nlist_cap = nlist_cap
+    # Q = N T* (0.5)^2 in reduced units (the Q_in of the deck times m sigma^2)
+    c.Q = q if q is not None else n * temp * 0.25
+    return c
+
+
+def init_random(n, box, rmin, kt_over_m, seed):
+    """Seeded start: positions uniform with all pairs >= rmin apart,
+    Maxwell-Boltzmann velocities (host code in libclmd.so)."""
+    lib = load()
+    arrs = [np.zeros(n) for _ in range(6)]
+    bx, by, bz = box
+    st = lib.clmd_init_random(n, bx, by, bz, rmin, kt_over_m, seed,
+                              *[ptr(a, C.c_double) for a in arrs])
+    if st:
+        raise ClmdError(st, "clmd_init_random")
+    x, y, z, vx, vy, vz = arrs
+    return x, y, z, vx, vy, vz
+
+
+def scalars_init(cfg: Config) -> Scalars:
+    s = Scalars()
+    load().clmd_scalars_init(C.byref(cfg), C.byref(s))
+    return s
+
+
+@dataclass
+class State:
+    x: np.ndarray
+    y: np.ndarray
+    z: np.ndarray
+    vx: np.ndarray
+    vy: np.ndarray
+    vz: np.ndarray
+    ax: np.ndarray
+    ay: np.ndarray
+    az: np.ndarray
+
+    def copy(self):
+        return State(*[getattr(self, k).copy() for k in self.__dataclass_fields__])
+
+    def arrays(self):
+        return [getattr(self, k) for k in self.__dataclass_fields__]
+
+
+class System:
+    """One device-resident system (clmd_system*)."""
+
+    def __init__(self, cfg: Config):
+        self.lib = load()
+        self.cfg = cfg
+        self.n = cfg.natom
+        h = C.c_void_p()
+        st = self.lib.clmd_create(C.byref(cfg), C.byref(h))
+        if st:
+            raise ClmdError(st, "clmd_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.clmd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, st, what):
+        if st not in (OK,) and st > ERR_BAD_SPECIES:
+            raise ClmdError(st, what)
+        return st
+
+    # -- state -------------------------------------------------------------
+    def set_state(self, state: State | None = None, api=None, scalars: Scalars | None = None):
+        arrs = state.arrays() if state is not None else [None] * 9
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) if a is not None else None
+                for a in arrs]
+        a = np.ascontiguousarray(api, dtype=np.int32) if api is not None else None
+        st = self.lib.clmd_set_state(self.h, *[ptr(v, C.c_double) for v in arrs],
+                                     ptr(a, C.c_int32),
+                                     C.byref(scalars) if scalars is not None else None)
+        return self._chk(st, "clmd_set_state")
+
+    def get_state(self) -> State:
+        arrs = [np.zeros(self.n) for _ in range(9)]
+        st = self.lib.clmd_get_state(self.h, *[ptr(v, C.c_double) for v in arrs], None)
+        self._chk(st, "clmd_get_state")
+        return State(*arrs)
+
+    def scalars(self) -> Scalars:
+        s = Scalars()
+        self._chk(self.lib.clmd_get_scalars(self.h, C.byref(s)), "clmd_get_scalars")
+        return s
+
+    def set_scalars(self, s: Scalars):
+        return self._chk(self.lib.clmd_set_scalars(self.h, C.byref(s)), "clmd_set_scalars")
+
+    def clear_status(self):
+        return self.lib.clmd_clear_status(self.h)
+
+    # -- the reference's subroutines ------------------------------------------
+    def neighbor(self, step):
+        s = C.c_int32(step)
+        st = self._chk(self.lib.clmd_neighbor(self.h, C.byref(s)), "neighbor")
+        return st, s.value
+
+    def accatom(self):
+        return self._chk(self.lib.clmd_accatom(self.h), "accatom")
+
+    def accwall(self):
+        return self._chk(self.lib.clmd_accwall(self.h), "accwall")
+
+    def zero_acc(self):
+        return self._chk(self.lib.clmd_zero_acc(self.h), "zero_acc")
+
+    def integrator(self, step):
+        return self._chk(self.lib.clmd_integrator(self.h, step), "integrator")
+
+    def thermostat(self, step):
+        return self._chk(self.lib.clmd_thermostat(self.h, step), "thermostat")
+
+    def stopdead(self, step):
+        return self._chk(self.lib.clmd_stopdead(self.h, step), "stopdead")
+
+    def stoddard(self, step):
+        return self._chk(self.lib.clmd_stoddard(self.h, step), "stoddard")
+
+    def chk_nucleation(self, step):
+        s = C.c_int32(step)
+        st = self._chk(self.lib.clmd_chk_nucleation(self.h, C.byref(s)), "chk_nucleation")
+        return st, s.value
+
+    def run(self, first, nsteps):
+        nxt = C.c_int32(0)
+        st = self._chk(self.lib.clmd_run(self.h, first, nsteps, C.byref(nxt)), "run")
+        return st, nxt.value
+
+    def synchronize(self):
+        return self._chk(self.lib.clmd_synchronize(self.h), "synchronize")
+
+    def stream(self):
+        return self.lib.clmd_stream(self.h)
+
+    def kernel_launches(self):
+        return self.lib.clmd_kernel_launches(self.h)
+
+    # -- outputs -------------------------------------------------------------
+    def halflist(self):
+        """(atnlist, atnidx) in the reference's layout (1-based values)."""
+        n = C.c_int64(0)
+        self._chk(self.lib.clmd_get_halflist(self.h, None, 0, None, C.byref(n)), "halflist")
+        lst = np.zeros(max(n.value, 1), dtype=np.int32)
+        idx = np.zeros(self.n, dtype=np.int32)
+        self._chk(self.lib.clmd_get_halflist(self.h, ptr(lst, C.c_int32), n.value,
+                                             ptr(idx, C.c_int32), C.byref(n)), "halflist")
+        return lst[: n.value], idx
+
+    def clusters(self) -> dict:
+        out = {}
+        v = ClusterView()
+        for name, dt, kind in CLUSTER_FIELDS:
+            a = np.zeros(self.n + (1 if kind == "N1" else 0), dtype=dt)
+            out[name] = a
+            setattr(v, name, ptr(a, C.c_int32 if dt == np.int32 else C.c_double))
+        self._chk(self.lib.clmd_get_clusters(self.h, C.byref(v)), "clusters")
+        return out

@@ -1,0 +1,170 @@
+// clmd_internal.cuh -- device state layout, launch parameters and reduction
+// helpers shared by the engine's CUDA translation units.
+//
+// Data layout in HBM (one system):
+//   pos    double4[N]  x, y, z, w = species (as double); packed so that a
+//                      neighbour gather is one 32-byte sector
+//   vx..vz double[N]   SoA, like /ATOMC/ x1,y1,z1
+//   ax..az double[N]   SoA, like /ATOMC/ x2,y2,z2
+//   list   int32[cap]  full Verlet list in CSR rows (0-based atom indices,
+//                      each row ascending); rows are placed by a warp-
+//                      aggregated cursor, row_start/row_len/row_lo index them
+//   cells  counting-sort bins: cell_count/start/fill, cell_atoms, spos
+//   DevState           scalars (clmd_scalars first, so the host copies it
+//                      with one memcpy), reduction counters, grid geometry
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/clmd.h"
+
+namespace clmd {
+
+constexpr int kBlock = 256;        // threads per block of the per-atom kernels
+constexpr int kMaxRedBlocks = 4096; // partial-sum slots per reduction
+constexpr int kScanTile = 2048;    // counts per block of the cell scan
+
+// LJ coefficients by ij = api(i)+api(j) (for-a-lj-n-pbc-m.f:61-76,119-131):
+// index 2 = species 1-1, 3 = 1-2, 4 = 2-2.
+struct Params {
+  double apmas[CLMD_MXSORTS];
+  double boxx, boxy, boxz, ibx, iby, ibz;
+  double dt, atrcut, atr2, atskin2, sig1;
+  double c1[5], c2[5], c3[5], eps[5];
+  double Q, att;
+  double nkt3_i;  // 3*natom*cikb*att with 3*natom an INTEGER product
+  double nkt3_d;  // 3.0d0*natom*cikb*att
+  double ekinT[CLMD_MXSORTS];  // 1.5d0*cikb*att*apnum(s)
+  int N, atsorts;
+  int apnum[CLMD_MXSORTS];
+  int sp_start[CLMD_MXSORTS + 1];  // first atom (0-based) of each species block
+  int nbtim, btim, atnenum, csover, clwait, ftcsi;
+  int ncx_max, ncy_max, ncz_max;
+  int list_cap;
+  int integrator, clustering;
+  char apth[CLMD_MXSORTS];
+  char ethst, clnuctrl;
+};
+
+struct DevState {
+  clmd_scalars s;               // must stay first: copied to the host as is
+  unsigned long long dmax2;     // max displacement^2 bits (atomicMax)
+  unsigned long long list_used; // CSR cursor
+  int rebuild;                  // this step rebuilds the list
+  int cur_step;                 // the reference's loop counter i
+  int err_new;                  // error raised inside a kernel, merged later
+  int ncx, ncy, ncz, ncell;
+  int nox, noy, noz;
+  int offx[3], offy[3], offz[3];
+  double cfx, cfy, cfz;         // cells per unit length
+  double rs2;
+  // thermostat
+  double kf[CLMD_MXSORTS];
+  int scale[CLMD_MXSORTS];
+  double vcom[3];
+  // clustering
+  int nroots, nliq, nroots_f;
+  int clu_force;                // next analysis runs even if cstep == step
+  unsigned int ctr[16];         // last-block counters (one per reduction site)
+  unsigned int bar_count, bar_gen;  // grid barrier of cooperative kernels
+};
+
+enum CtrSlot {
+  CTR_DRIFT = 0,
+  CTR_FORCE,
+  CTR_THERMO,
+  CTR_MOM,
+  CTR_MOM2,
+  CTR_CLU,
+  CTR_CLU2,
+  CTR_NHSOLVE,
+  CTR_SCAN,
+};
+
+__device__ __forceinline__ bool gated(const DevState* st) {
+  return st->s.status != 0 || st->s.aborted != 0;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Fixed-shape block sum (deterministic for a given block size); result valid
+// in thread 0.  sh must hold blockDim.x/32 doubles.
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (w == 0) {
+    r = lane < nw ? sh[lane] : 0.0;
+    r = warp_sum(r);
+  }
+  return r;
+}
+
+__device__ __forceinline__ double block_max(double v, double* sh) {
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  v = warp_max(v);
+  __syncthreads();
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (w == 0) {
+    r = lane < nw ? sh[lane] : 0.0;
+    r = warp_max(r);
+  }
+  return r;
+}
+
+// Returns true in every thread of the block that arrives last; that block
+// may then read all partials (written before the fence) with __ldcg.
+__device__ __forceinline__ bool last_block(unsigned int* ctr) {
+  __shared__ int am_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned int t = atomicAdd(ctr, 1u);
+    am_last = (t == gridDim.x - 1);
+    if (am_last) *ctr = 0u;
+  }
+  __syncthreads();
+  if (am_last) __threadfence();
+  return am_last != 0;
+}
+
+// Sum of n partials in a fixed order by one block (deterministic).
+__device__ __forceinline__ double reduce_partials(const double* p, int n, double* sh) {
+  double v = 0.0;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) v += __ldcg(p + k);
+  return block_sum(v, sh);
+}
+
+// The reference's minimum image for force and cluster distances
+// (for-a-lj-n-pbc-m.f:109-111): d + L*(bf1 - int(bf2 + d/L)).
+__device__ __forceinline__ double mimage_bf(double d, double L, double iL, double bf1,
+                                            double bf2) {
+  return d + L * (bf1 - (double)(int)(bf2 + d * iL));
+}
+
+// The neighbour-list minimum image (neighbor-pbc-mav.f:84-86).
+__device__ __forceinline__ double mimage_nb(double d, double L, double iL) {
+  return d + L - L * (double)(int)(1.5 + d * iL);
+}
+
+__device__ __forceinline__ void raise_err(DevState* st, int code) {
+  atomicCAS(&st->err_new, 0, code);
+}
+
+}  // namespace clmd

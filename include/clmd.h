@@ -1,0 +1,218 @@
+/*
+ * clmd.h -- C ABI of the B200 engine for the Lennard-Jones MD step and the
+ * cluster (nucleation) analysis of the Fortran 77 code "cluster"
+ * (janw76/fortran-cluster-md).
+ *
+ * Two surfaces are exported by libclmd.so:
+ *
+ *  1. The reference's own subroutine surface with gfortran name mangling
+ *     (lower case + trailing underscore), state passed through the common
+ *     blocks, so that the unchanged Fortran host (main.f, read-3d.f and the
+ *     writers) links against this library instead of the Fortran physics
+ *     files.  Declared in clmd_f77.h.
+ *
+ *  2. A handle based C API (clmd_*) with runtime sizes (no mxa limit) that
+ *     the F77 surface is built on, and that C/C++/Python hosts call directly.
+ *
+ * Conventions of the C API:
+ *  - per-atom arrays are 0-based in memory (atom i, 1-based as in the
+ *    reference, lives at element i-1); values that ARE atom indices (list
+ *    entries, cluster labels) keep the reference's 1-based numbering, so a
+ *    downloaded half list is byte-identical to the reference's atnlist();
+ *  - histograms indexed by cluster size (csi, csif, ceks, ...) have N+1
+ *    elements and are indexed by the size itself, as the reference's
+ *    csi(0:mxa);
+ *  - every function returns a CLMD_* status code; the first error seen on
+ *    the device is also latched in clmd_scalars.status and every later device
+ *    kernel of that system is a no-op until clmd_clear_status().
+ *
+ * Units are the reference's internal ones (length, mass, energy, time and
+ * Boltzmann's constant CLMD_CIKB as in const.inc); a reduced-unit run sets
+ * sigma = eps = m = 1 and att = T* / CLMD_CIKB.
+ */
+#ifndef CLMD_H
+#define CLMD_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* const.inc:10-18 */
+#define CLMD_MXA 6000
+#define CLMD_MXNLIST (CLMD_MXA * CLMD_MXA / 4)
+#define CLMD_MXSORTS 10
+#define CLMD_CIKB 1.38066e-6  /* Boltzmann constant, internal units */
+#define CLMD_CIMU 1.66056     /* atomic mass unit, internal units */
+
+/* status codes (the reference STOPs on 1-4) */
+#define CLMD_OK 0
+#define CLMD_ERR_SKIN 1           /* neighbor-pbc-mav.f:48-51 "Skin radius exceeded" */
+#define CLMD_ERR_LIST_OVERFLOW 2  /* neighbor-pbc-mav.f:94-98 "Neighborlist is nearly full" */
+#define CLMD_ERR_NH_NOCONVERGE 3  /* int-verlet-nh-mav.f:150-166 */
+#define CLMD_ERR_BAD_SPECIES 4    /* for-a-lj-n-pbc-m.f:129-130 "Nanu???" */
+#define CLMD_ERR_ARG 5            /* bad argument / size beyond a limit */
+#define CLMD_ERR_CUDA 6           /* a CUDA runtime call failed */
+#define CLMD_ERR_NOMEM 7          /* device allocation failed */
+#define CLMD_ERR_NO_DEVICE 8      /* no CUDA device: the engine has no CPU path */
+#define CLMD_ERR_TIMEOUT 9        /* a bounded device wait gave up */
+
+/* integrator variants (Makefile:45-88 pick these at link time) */
+#define CLMD_INT_VERLET 0 /* int-verlet-mav.f      (targets NUC/SILENT/FRENKEL) */
+#define CLMD_INT_NOSE 1   /* int-verlet-nh-mav.f   (target NOSE) */
+/* cluster analysis variants */
+#define CLMD_CLU_STILLINGER 0 /* stoddard-pbc-n-m.f     (targets NUC/SILENT/NOSE) */
+#define CLMD_CLU_FRENKEL 1    /* stoddard-pbc-n-m-fre.f (target FRENKEL) */
+/* arithmetic of the pair forces */
+#define CLMD_PREC_FP64 0  /* all FP64: bit-identical per-atom forces */
+#define CLMD_PREC_MIXED 1 /* FP32 pair terms, Kahan-compensated FP32 sums */
+
+/* Run parameters: the deck (.3d) fields of the hot path, after read-3d.f's
+ * unit conversion (read-3d.f:152-161, 246-261). */
+typedef struct clmd_config {
+  double apmas[CLMD_MXSORTS]; /* mass of species s */
+  double apsig[CLMD_MXSORTS]; /* LJ sigma of species s */
+  double apeps[CLMD_MXSORTS]; /* LJ epsilon of species s */
+  double att;                 /* system temperature */
+  double atskin;              /* cluster criterion radius (absolute) */
+  double atrcut;              /* potential cut-off radius (absolute) */
+  double atrskin;             /* initial neighbour-list radius (absolute) */
+  double Q;                   /* Nose-Hoover mass (already * m sigma^2) */
+  double boxx, boxy, boxz;    /* periodic box */
+  double dt;                  /* time step */
+  int64_t nlist_cap;          /* half-list entry capacity, 0 = automatic */
+  int32_t natom;              /* total atoms */
+  int32_t atsorts;            /* species count (1..CLMD_MXSORTS) */
+  int32_t apnum[CLMD_MXSORTS];/* atoms per species, contiguous, in order */
+  int32_t atnenum;            /* ten Wolde-Frenkel neighbour threshold */
+  int32_t nbtim;              /* target steps between list rebuilds */
+  int32_t btim;               /* first step number */
+  int32_t csover;             /* nucleation size threshold ("a cluster >= csover") */
+  int32_t clwait;             /* steps the cluster must persist */
+  int32_t ftcsi;              /* steps between cluster analyses (0 = never) */
+  int32_t integrator;         /* CLMD_INT_* */
+  int32_t clustering;         /* CLMD_CLU_* */
+  int32_t precision;          /* CLMD_PREC_* */
+  char apth[CLMD_MXSORTS];    /* 'X' = species thermostatted by velocity scaling */
+  char ethst;                 /* 'X' velocity scaling every step, 'N' Nose-Hoover, '-' none */
+  char clnuctrl;              /* 'X' = abort the run on nucleation */
+  char pad[4];
+} clmd_config;
+
+/* Dynamic scalars: the hot path's scalar members of /ENERG/, /ATOMP/,
+ * /DMMPP/ and /CVTPP/, plus engine bookkeeping. */
+typedef struct clmd_scalars {
+  double ekin, sumv2, epot, H;   /* energ.inc */
+  double psi, s, atrskin;        /* atomp.inc (atrskin adapts at rebuilds) */
+  double dmms, dmmsu, dmmax, dmmav;
+  double dmmh[256];              /* dmmpp.inc ring of max displacements */
+  double virial;                 /* sum over pairs of f_ij r_ij^2 (not in the reference) */
+  int64_t npairs_half;           /* half-list entries after the last rebuild */
+  int32_t dmmst, dmmi;
+  int32_t clbrkt, cnum, cnumf, cstep;
+  int32_t cbiggest, cbiggestf, clookfor, clookforf;
+  int32_t status;                /* first error, CLMD_OK if none */
+  int32_t fail_step;             /* step at which status was set */
+  int32_t nh_iters;              /* sweeps of the last Nose-Hoover velocity solve */
+  int32_t nrebuild;              /* neighbour-list rebuilds so far */
+  int32_t last_rebuild_step;
+  int32_t aborted;               /* chk_nucleation negated the step */
+  int32_t maxcs;                 /* largest Stillinger cluster of the last analysis */
+  int32_t pad;
+} clmd_scalars;
+
+/* Cluster-analysis outputs (cvtpp.inc).  Any pointer may be NULL.
+ * Sizes: cl, clf: N.  cs, cek, cgs, cgsa, cfpt, cfptf: N, element k-1 holds
+ * the reference's index k.  csi, csif, ceks, ceksf, csf, cekf, cgsf, cgsfa:
+ * N+1, indexed like the reference's (0:mxa) arrays. */
+typedef struct clmd_cluster_view {
+  int32_t *cl, *cs, *csi;
+  double *cek, *ceks;
+  int32_t *clf, *csf, *csif;
+  double *cekf, *ceksf;
+  int32_t *cgs, *cgsa, *cgsf, *cgsfa;
+  int32_t *cfpt, *cfptf;
+} clmd_cluster_view;
+
+/* Fills the scalars a fresh run starts from: read-3d.f:263-276 (dmm ring,
+ * first-passage cursors) and main.f:156-166 (Nose-Hoover start values need
+ * ekin, so psi is left at 0 here). */
+void clmd_scalars_init(const clmd_config* cfg, clmd_scalars* sc);
+
+typedef struct clmd_system clmd_system;
+
+/* Allocates the device state of one system on the current CUDA device.
+ * Returns CLMD_ERR_NO_DEVICE when no GPU is visible (there is no CPU path). */
+int clmd_create(const clmd_config* cfg, clmd_system** out);
+int clmd_destroy(clmd_system* sys);
+
+/* Host <-> device state.  Any array pointer may be NULL (not copied).
+ * api is the 1-based species of each atom (atomp.inc api()). */
+int clmd_set_state(clmd_system* sys, const double* x, const double* y, const double* z,
+                   const double* vx, const double* vy, const double* vz,
+                   const double* ax, const double* ay, const double* az,
+                   const int32_t* api, const clmd_scalars* sc);
+int clmd_get_state(clmd_system* sys, double* x, double* y, double* z,
+                   double* vx, double* vy, double* vz,
+                   double* ax, double* ay, double* az, clmd_scalars* sc);
+int clmd_get_scalars(clmd_system* sys, clmd_scalars* sc);
+int clmd_set_scalars(clmd_system* sys, const clmd_scalars* sc);
+int clmd_clear_status(clmd_system* sys);
+
+/* The reference's subroutines, one call each (all enqueue on the system's
+ * stream; the *_sync variants of the F77 shim wait).  step follows the
+ * reference: neighbor() flips a negative step to positive. */
+int clmd_neighbor(clmd_system* sys, int32_t* step);        /* neighbor-pbc-mav.f:13-109 */
+int clmd_accatom(clmd_system* sys);                        /* for-a-lj-n-pbc-m.f:18-154 */
+int clmd_accwall(clmd_system* sys);                        /* for-w-dummy.f:9-14 */
+int clmd_zero_acc(clmd_system* sys);                       /* int-verlet-mav.f:76-81 */
+int clmd_integrator(clmd_system* sys, int32_t step);       /* int-verlet-mav.f / int-verlet-nh-mav.f */
+int clmd_thermostat(clmd_system* sys, int32_t step);       /* scalev-nh-m.f:19-81 */
+int clmd_stopdead(clmd_system* sys, int32_t step);         /* stopdead-m.f:10-78 */
+int clmd_stoddard(clmd_system* sys, int32_t step);         /* stoddard-pbc-n-m[-fre].f */
+int clmd_chk_nucleation(clmd_system* sys, int32_t* step);  /* chk-nucleation.f:15-58 */
+
+/* main.f:177-228 loop body for steps first..first+nsteps-1, device-resident:
+ * [stoddard every ftcsi] -> [thermostat if ethst=='X'] ->
+ * [chk_nucleation every ftcsi if clnuctrl=='X'] -> integrator.  Replays
+ * captured CUDA graphs.  *next_step gets the loop counter after the run
+ * (negative if chk_nucleation aborted, as main.f:219-220). */
+int clmd_run(clmd_system* sys, int32_t first, int32_t nsteps, int32_t* next_step);
+
+/* The half neighbour list in the reference's layout (atomp.inc atnlist():
+ * header -i, then the j>i neighbours ascending) and atnidx().  cap is the
+ * capacity of atnlist in entries; *nentries gets the used length. */
+int clmd_get_halflist(clmd_system* sys, int32_t* atnlist, int64_t cap,
+                      int32_t* atnidx, int64_t* nentries);
+int clmd_get_clusters(clmd_system* sys, const clmd_cluster_view* view);
+
+/* Waits for the system's stream. */
+int clmd_synchronize(clmd_system* sys);
+/* Enqueue-only timing helpers: the CUDA stream the system launches on. */
+void* clmd_stream(clmd_system* sys);
+/* Number of kernels this system has launched (graph replays count each
+ * kernel node). */
+int64_t clmd_kernel_launches(clmd_system* sys);
+
+/* Seeded synthetic start configuration (not part of the reference's hot
+ * path): positions uniform in the box with every pair at least rmin apart
+ * (random sequential addition on a cell grid), Maxwell-Boltzmann velocities
+ * at temperature kT for mass m (unit-free: v = sqrt(kT/m) * N(0,1)).
+ * Returns CLMD_ERR_ARG if the packing is too dense to finish. */
+int clmd_init_random(int32_t n, double boxx, double boxy, double boxz, double rmin,
+                     double kT_over_m, uint64_t seed, double* x, double* y, double* z,
+                     double* vx, double* vy, double* vz);
+
+const char* clmd_status_string(int status);
+/* sizeof of the ABI structs (0 config, 1 scalars, 2 cluster view), so that
+ * bindings in other languages can check their layout. */
+int64_t clmd_struct_size(int which);
+/* Last status returned by any clmd_* or F77 entry point of this process. */
+int32_t clmd_last_status(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CLMD_H */
