@@ -173,9 +173,14 @@ extern "C" int clmd_create(const clmd_config* cfg, clmd_system** out) {
   size_t naux = std::max<size_t>((size_t)ntiles, (size_t)S->nblk) + 64;
 
   CK(dalloc(&S->pos, N));
+  CK(dalloc(&S->pos_alt, N));
   CK(dalloc(&S->vx, N)); CK(dalloc(&S->vy, N)); CK(dalloc(&S->vz, N));
   CK(dalloc(&S->ax, N)); CK(dalloc(&S->ay, N)); CK(dalloc(&S->az, N));
   CK(dalloc(&S->api, N));
+  CK(dalloc(&S->perm, N)); CK(dalloc(&S->iperm, N)); CK(dalloc(&S->perm_s, N));
+  CK(dalloc(&S->pos_s, N));
+  CK(dalloc(&S->vx_s, N)); CK(dalloc(&S->vy_s, N)); CK(dalloc(&S->vz_s, N));
+  CK(dalloc(&S->ax_s, N)); CK(dalloc(&S->ay_s, N)); CK(dalloc(&S->az_s, N));
   CK(dalloc(&S->sx, N)); CK(dalloc(&S->sy, N)); CK(dalloc(&S->sz, N));
   CK(dalloc(&S->vxn, N)); CK(dalloc(&S->vyn, N)); CK(dalloc(&S->vzn, N));
   CK(dalloc(&S->list, (size_t)cap));
@@ -185,9 +190,10 @@ extern "C" int clmd_create(const clmd_config* cfg, clmd_system** out) {
   CK(dalloc(&S->cell_fill, S->ncell_alloc + 1));
   CK(dalloc(&S->cell_atoms, N));
   CK(dalloc(&S->atom_cell, N));
-  CK(dalloc(&S->spos, N));
   CK(dalloc(&S->scan_aux, naux));
   CK(dalloc(&S->partials, npart));
+  S->cyc_blocks = cycle_blocks_for(S);
+  CK(dalloc(&S->red, (size_t)2 * 16 * S->cyc_blocks + 64));
   CK(dalloc(&S->st, 1));
   CK(cudaMallocHost((void**)&S->h_sc, sizeof(clmd_scalars)));
   CK(dalloc(&S->parent, N)); CK(dalloc(&S->parent2, N));
@@ -200,7 +206,7 @@ extern "C" int clmd_create(const clmd_config* cfg, clmd_system** out) {
   CK(dalloc(&S->cek, N)); CK(dalloc(&S->cekf, N + 1));
   CK(dalloc(&S->ceks, N + 1)); CK(dalloc(&S->ceksf, N + 1));
   CK(dalloc(&S->deg, N)); CK(dalloc(&S->deg1, N));
-  CK(dalloc(&S->liq, N)); CK(dalloc(&S->liqrank, N));
+  CK(dalloc(&S->liq, N)); CK(dalloc(&S->liqrank, N)); CK(dalloc(&S->liqref, N));
   CK(dalloc(&S->bonds, (size_t)S->bond_cap));
   CK(dalloc(&S->nbonds, 1));
 
@@ -216,6 +222,7 @@ extern "C" int clmd_create(const clmd_config* cfg, clmd_system** out) {
   CK(cudaMemsetAsync(S->cek, 0, sizeof(double) * N, S->stream));
   double* dz1[] = {S->cekf, S->ceks, S->ceksf};
   for (double* p : dz1) CK(cudaMemsetAsync(p, 0, sizeof(double) * (N + 1), S->stream));
+  CK(cudaMemsetAsync(S->cell_count, 0, sizeof(int) * (S->ncell_alloc + 1), S->stream));
   CK(cudaMemsetAsync(S->cfpt, 0xff, sizeof(int) * N, S->stream));
   CK(cudaMemsetAsync(S->cfptf, 0xff, sizeof(int) * N, S->stream));
   // species from the contiguous blocks (read-3d.f:249-252)
@@ -224,11 +231,15 @@ extern "C" int clmd_create(const clmd_config* cfg, clmd_system** out) {
   for (int s = 0; s < cfg->atsorts; s++)
     for (int j = 0; j < cfg->apnum[s]; j++) api[n++] = s + 1;
   CK(cudaMemcpyAsync(S->api, api.data(), sizeof(int) * N, cudaMemcpyHostToDevice, S->stream));
+  // storage starts in reference order
+  std::vector<int> ident(N);
+  for (int i = 0; i < N; i++) ident[i] = i;
+  CK(cudaMemcpy(S->perm, ident.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(S->iperm, ident.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
   clmd_scalars_init(cfg, S->h_sc);
   CK(cudaMemcpyAsync(&S->st->s, S->h_sc, sizeof(clmd_scalars), cudaMemcpyHostToDevice,
                      S->stream));
-  pack_pos_launch(S, 0, 0, 0);
-  S->coop_blocks = coop_blocks_for(S);
+  scatter_in_launch(S, 0, 0, 0, 0, 0, 0, 0, 0, 0);
   CK(cudaStreamSynchronize(S->stream));
   CK(cudaGetLastError());
   *out = S;
@@ -237,8 +248,7 @@ extern "C" int clmd_create(const clmd_config* cfg, clmd_system** out) {
 
 static void free_graphs(clmd_system* S) {
   if (S->cyc_exec) cudaGraphExecDestroy(S->cyc_exec);
-  if (S->step_exec) cudaGraphExecDestroy(S->step_exec);
-  S->cyc_exec = S->step_exec = nullptr;
+  S->cyc_exec = nullptr;
   S->graphs_ok = false;
 }
 
@@ -246,10 +256,12 @@ extern "C" int clmd_destroy(clmd_system* S) {
   if (!S) return CLMD_OK;
   cudaStreamSynchronize(S->stream);
   free_graphs(S);
-  void* ps[] = {S->pos, S->vx, S->vy, S->vz, S->ax, S->ay, S->az, S->api, S->sx, S->sy,
+  void* ps[] = {S->pos, S->pos_alt, S->red, S->vx, S->vy, S->vz, S->ax, S->ay, S->az, S->api, S->perm, S->iperm,
+                S->perm_s, S->pos_s, S->vx_s, S->vy_s, S->vz_s, S->ax_s, S->ay_s, S->az_s,
+                S->liqref, S->sx, S->sy,
                 S->sz, S->vxn, S->vyn, S->vzn, S->list, S->row_start, S->row_len, S->row_lo,
                 S->cell_count, S->cell_start, S->cell_fill, S->cell_atoms, S->atom_cell,
-                S->spos, S->scan_aux, S->partials, S->st, S->parent, S->parent2, S->cl,
+                S->scan_aux, S->partials, S->st, S->parent, S->parent2, S->cl,
                 S->clf, S->cs, S->csf, S->csi, S->csif, S->cgs, S->cgsf, S->cgsa, S->cgsfa,
                 S->cfpt, S->cfptf, S->cek, S->cekf, S->ceks, S->ceksf, S->deg, S->deg1,
                 S->liq, S->liqrank, S->bonds, S->nbonds};
@@ -284,21 +296,24 @@ extern "C" int clmd_set_state(clmd_system* S, const double* x, const double* y,
       if (api[i] < 1 || api[i] > S->P.atsorts) return set_last(CLMD_ERR_ARG);
     CK(cudaMemcpyAsync(S->api, api, sizeof(int) * S->P.N, cudaMemcpyHostToDevice, s));
   }
-  if (x) CK(cudaMemcpyAsync(S->sx, x, nb, cudaMemcpyHostToDevice, s));
-  if (y) CK(cudaMemcpyAsync(S->sy, y, nb, cudaMemcpyHostToDevice, s));
-  if (z) CK(cudaMemcpyAsync(S->sz, z, nb, cudaMemcpyHostToDevice, s));
-  if (x || y || z || api) pack_pos_launch(S, x != nullptr, y != nullptr, z != nullptr);
-  if (vx) CK(cudaMemcpyAsync(S->vx, vx, nb, cudaMemcpyHostToDevice, s));
-  if (vy) CK(cudaMemcpyAsync(S->vy, vy, nb, cudaMemcpyHostToDevice, s));
-  if (vz) CK(cudaMemcpyAsync(S->vz, vz, nb, cudaMemcpyHostToDevice, s));
-  if (ax) CK(cudaMemcpyAsync(S->ax, ax, nb, cudaMemcpyHostToDevice, s));
-  if (ay) CK(cudaMemcpyAsync(S->ay, ay, nb, cudaMemcpyHostToDevice, s));
-  if (az) CK(cudaMemcpyAsync(S->az, az, nb, cudaMemcpyHostToDevice, s));
+  const double* src[9] = {x, y, z, vx, vy, vz, ax, ay, az};
+  double* stg[9] = {S->sx, S->sy, S->sz, S->vx_s, S->vy_s, S->vz_s, S->ax_s, S->ay_s, S->az_s};
+  bool any = api != nullptr;
+  for (int k = 0; k < 9; k++)
+    if (src[k]) {
+      CK(cudaMemcpyAsync(stg[k], src[k], nb, cudaMemcpyHostToDevice, s));
+      any = true;
+    }
+  if (any)
+    scatter_in_launch(S, x != nullptr, y != nullptr, z != nullptr, vx != nullptr,
+                      vy != nullptr, vz != nullptr, ax != nullptr, ay != nullptr,
+                      az != nullptr);
   if (sc) {
     *S->h_sc = *sc;
     CK(cudaMemcpyAsync(&S->st->s, S->h_sc, sizeof(clmd_scalars), cudaMemcpyHostToDevice, s));
   }
   CK(cudaStreamSynchronize(s));
+  CK(cudaGetLastError());
   return set_last(CLMD_OK);
 }
 
@@ -308,16 +323,13 @@ extern "C" int clmd_get_state(clmd_system* S, double* x, double* y, double* z, d
   if (!S) return set_last(CLMD_ERR_ARG);
   const size_t nb = sizeof(double) * S->P.N;
   cudaStream_t s = S->stream;
-  if (x || y || z) unpack_pos_launch(S);
-  if (x) CK(cudaMemcpyAsync(x, S->sx, nb, cudaMemcpyDeviceToHost, s));
-  if (y) CK(cudaMemcpyAsync(y, S->sy, nb, cudaMemcpyDeviceToHost, s));
-  if (z) CK(cudaMemcpyAsync(z, S->sz, nb, cudaMemcpyDeviceToHost, s));
-  if (vx) CK(cudaMemcpyAsync(vx, S->vx, nb, cudaMemcpyDeviceToHost, s));
-  if (vy) CK(cudaMemcpyAsync(vy, S->vy, nb, cudaMemcpyDeviceToHost, s));
-  if (vz) CK(cudaMemcpyAsync(vz, S->vz, nb, cudaMemcpyDeviceToHost, s));
-  if (ax) CK(cudaMemcpyAsync(ax, S->ax, nb, cudaMemcpyDeviceToHost, s));
-  if (ay) CK(cudaMemcpyAsync(ay, S->ay, nb, cudaMemcpyDeviceToHost, s));
-  if (az) CK(cudaMemcpyAsync(az, S->az, nb, cudaMemcpyDeviceToHost, s));
+  double* dst[9] = {x, y, z, vx, vy, vz, ax, ay, az};
+  double* stg[9] = {S->sx, S->sy, S->sz, S->vx_s, S->vy_s, S->vz_s, S->ax_s, S->ay_s, S->az_s};
+  bool any = false;
+  for (int k = 0; k < 9; k++) any = any || dst[k];
+  if (any) gather_out_launch(S);
+  for (int k = 0; k < 9; k++)
+    if (dst[k]) CK(cudaMemcpyAsync(dst[k], stg[k], nb, cudaMemcpyDeviceToHost, s));
   int st = fetch(S);
   if (sc) *sc = *S->h_sc;
   return st == CLMD_OK || st > 0 ? set_last(CLMD_OK) : st;
@@ -352,6 +364,7 @@ __global__ void k_merge_err(DevState* st) {
 
 extern "C" int clmd_clear_status(clmd_system* S) {
   if (!S) return set_last(CLMD_ERR_ARG);
+  clear_cells(S);  // a rebuild cut short by an error may have left counts
   k_clear_status<<<1, 1, 0, S->stream>>>(S->st);
   S->launches++;
   return fetch(S);
@@ -360,10 +373,7 @@ extern "C" int clmd_clear_status(clmd_system* S) {
 extern "C" int clmd_neighbor(clmd_system* S, int32_t* step) {
   if (!S || !step) return set_last(CLMD_ERR_ARG);
   k_set_step_launch(S, *step);
-  nb_prologue_launch(S);
-  rebuild_launch(S, S->stream);
-  k_merge_err<<<1, 1, 0, S->stream>>>(S->st);
-  S->launches++;
+  cycle_launch(S, 0, 1);
   if (*step < 0) *step = -*step;  // neighbor-pbc-mav.f:63
   return fetch(S);
 }
@@ -385,45 +395,10 @@ extern "C" int clmd_zero_acc(clmd_system* S) {
   return fetch(S);
 }
 
-static void enqueue_integrator(clmd_system* S, unsigned long long cond, int use_cond,
-                               bool capture) {
-  drift_launch(S, cond, use_cond);
-  if (!capture) rebuild_launch(S, S->stream);
-  else {
-    // conditional node around the rebuild kernels
-    cudaStreamCaptureStatus cs;
-    cudaGraph_t g;
-    const cudaGraphNode_t* deps = nullptr;
-    size_t ndeps = 0;
-    cudaStreamGetCaptureInfo(S->stream, &cs, nullptr, &g, &deps, &ndeps);
-    cudaGraphNodeParams cp = {};
-    cp.type = cudaGraphNodeTypeConditional;
-    cp.conditional.handle = (cudaGraphConditionalHandle)cond;
-    cp.conditional.type = cudaGraphCondTypeIf;
-    cp.conditional.size = 1;
-    cudaGraphNode_t node;
-    cudaGraphAddNode(&node, g, deps, ndeps, &cp);
-    cudaStreamUpdateCaptureDependencies(S->stream, &node, 1, cudaStreamSetCaptureDependencies);
-    cudaGraph_t body = cp.conditional.phGraph_out[0];
-    cudaStreamBeginCaptureToGraph(S->side, body, nullptr, nullptr, 0,
-                                  cudaStreamCaptureModeRelaxed);
-    long long before = S->launches;
-    rebuild_launch(S, S->side);
-    S->launches = before;  // body kernels run only on rebuild steps
-    cudaStreamEndCapture(S->side, &body);
-  }
-  if (S->P.integrator == CLMD_INT_NOSE) {
-    force_launch(S, FORCE_ZERO_FIRST);
-    nh_solve_launch(S);
-  } else {
-    force_launch(S, FORCE_VV_KICK);
-  }
-}
-
 extern "C" int clmd_integrator(clmd_system* S, int32_t step) {
   if (!S) return set_last(CLMD_ERR_ARG);
   k_set_step_launch(S, step);
-  enqueue_integrator(S, 0, 0, false);
+  cycle_launch(S, 1, 0);
   return fetch(S);
 }
 
@@ -455,46 +430,29 @@ extern "C" int clmd_chk_nucleation(clmd_system* S, int32_t* step) {
   return st;
 }
 
-// one main-loop step (main.f:179-226 with the writers off)
-static void enqueue_step(clmd_system* S, bool analysis, unsigned long long cond, int use_cond,
-                         bool capture) {
+// main.f:179-226 with the writers off, for the steps first..first+n-1 of
+// one analysis cycle: wrtCSI's stoddard at an analysis step (wrt-csi.f:27),
+// chk_nucleation, then the steps (velocity scaling inside the step kernel
+// when ethst == 'X', main.f:207).
+static void enqueue_cycle(clmd_system* S, bool analysis, int nsteps) {
   const clmd_config& c = S->cfg;
   if (analysis && c.ftcsi != 0) stoddard_launch(S, 0);
-  if (c.ethst == 'X') thermostat_launch(S, -2);  // any step value other than -1
   if (analysis && c.clnuctrl == 'X' && c.ftcsi != 0) chk_nucleation_launch(S);
-  enqueue_integrator(S, cond, use_cond, capture);
-  k_step_advance_launch(S);
-}
-
-static int capture_graph(clmd_system* S, int nsteps, bool analysis_first, cudaGraphExec_t* out,
-                         long long* kernels) {
-  cudaGraph_t g;
-  CK(cudaGraphCreate(&g, 0));
-  std::vector<cudaGraphConditionalHandle> hs(nsteps);
-  for (int k = 0; k < nsteps; k++)
-    CK(cudaGraphConditionalHandleCreate(&hs[k], g, 0, cudaGraphCondAssignDefault));
-  CK(cudaStreamBeginCaptureToGraph(S->stream, g, nullptr, nullptr, 0,
-                                   cudaStreamCaptureModeRelaxed));
-  long long before = S->launches;
-  for (int k = 0; k < nsteps; k++)
-    enqueue_step(S, analysis_first && k == 0, (unsigned long long)hs[k], 1, true);
-  *kernels = S->launches - before;
-  S->launches = before;
-  cudaGraph_t cap;
-  CK(cudaStreamEndCapture(S->stream, &cap));
-  cudaError_t e = cudaGraphInstantiate(out, g, 0);
-  cudaGraphDestroy(g);
-  CK(e);
-  return CLMD_OK;
+  if (nsteps > 0) cycle_launch(S, nsteps, 0);
 }
 
 static int ensure_graphs(clmd_system* S) {
-  if (S->graphs_ok) return CLMD_OK;
-  int cyc = S->cfg.ftcsi > 0 ? S->cfg.ftcsi : 100;
-  int r = capture_graph(S, cyc, S->cfg.ftcsi > 0, &S->cyc_exec, &S->cyc_kernels);
-  if (r) return r;
-  r = capture_graph(S, 1, false, &S->step_exec, &S->step_kernels);
-  if (r) return r;
+  if (S->graphs_ok || S->cfg.ftcsi <= 0) return CLMD_OK;
+  cudaGraph_t g;
+  CK(cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeRelaxed));
+  long long before = S->launches;
+  enqueue_cycle(S, true, S->cfg.ftcsi);
+  S->cyc_kernels = S->launches - before;
+  S->launches = before;
+  CK(cudaStreamEndCapture(S->stream, &g));
+  cudaError_t e = cudaGraphInstantiate(&S->cyc_exec, g, 0);
+  cudaGraphDestroy(g);
+  CK(e);
   S->graphs_ok = true;
   return CLMD_OK;
 }
@@ -505,31 +463,25 @@ extern "C" int clmd_run(clmd_system* S, int32_t first, int32_t nsteps, int32_t* 
   if (r) return set_last(r);
   k_set_step_launch(S, first);
   const int f = S->cfg.ftcsi;
-  int cyc = f > 0 ? f : 100;
   long long i = first, left = nsteps;
   while (left > 0) {
-    bool aligned = f > 0 ? (i % f == 0) : true;
-    if (aligned && left >= cyc) {
-      CK(cudaGraphLaunch(S->cyc_exec, S->stream));
+    if (f > 0 && i % f == 0 && left >= f) {
+      CK(cudaGraphLaunch(S->cyc_exec, S->stream));  // a whole analysis cycle
       S->launches += S->cyc_kernels;
-      i += cyc;
-      left -= cyc;
-    } else if (f > 0 && i % f == 0) {
-      // analysis step outside a full cycle: enqueue directly
-      enqueue_step(S, true, 0, 0, false);
-      i++;
-      left--;
-    } else {
-      CK(cudaGraphLaunch(S->step_exec, S->stream));
-      S->launches += S->step_kernels;
-      i++;
-      left--;
+      i += f;
+      left -= f;
+      continue;
     }
+    // a partial cycle: up to the next analysis step
+    bool analysis = f > 0 && i % f == 0;
+    long long n = f > 0 ? (f - (i % f + f) % f) : left;
+    if (n > left) n = left;
+    enqueue_cycle(S, analysis, (int)n);
+    i += n;
+    left -= n;
   }
   int st = fetch(S);
   if (next_step) {
-    int cs = S->h_sc ? 0 : 0;
-    (void)cs;
     int cur = 0;
     CK(cudaMemcpy(&cur, &S->st->cur_step, sizeof(int), cudaMemcpyDeviceToHost));
     *next_step = S->h_sc->aborted ? -cur : cur;
@@ -537,30 +489,42 @@ extern "C" int clmd_run(clmd_system* S, int32_t first, int32_t nsteps, int32_t* 
   return st;
 }
 
-__global__ void k_halflist(int N, const int* list, const int* row_start, const int* row_len,
-                           const int* row_lo, const long long* hstart, int* out) {
+// row of reference atom i: header -(i+1), then the j>i neighbours ascending
+__global__ void k_halflist(int N, const int* iperm, const int* perm, const int* list,
+                           const int* row_start, const int* row_len, const int* row_lo,
+                           const long long* hstart, int* out) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
+  int p = iperm[i];
   long long o = hstart[i];
   out[o] = -(i + 1);
-  int k0 = row_start[i] + row_lo[i], k1 = row_start[i] + row_len[i];
-  for (int k = k0; k < k1; k++) out[++o] = list[k] + 1;
+  int k0 = row_start[p] + row_lo[p], k1 = row_start[p] + row_len[p];
+  for (int k = k0; k < k1; k++) out[++o] = perm[list[k]] + 1;
+}
+
+__global__ void k_rowlens(int N, const int* iperm, const int* row_len, const int* row_lo,
+                          int* half) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  int p = iperm[i];
+  half[i] = row_len[p] - row_lo[p];
 }
 
 extern "C" int clmd_get_halflist(clmd_system* S, int32_t* atnlist, int64_t cap,
                                  int32_t* atnidx, int64_t* nentries) {
   if (!S) return set_last(CLMD_ERR_ARG);
   const int N = S->P.N;
-  std::vector<int> len(N), lo(N);
-  CK(cudaMemcpyAsync(len.data(), S->row_len, sizeof(int) * N, cudaMemcpyDeviceToHost,
+  std::vector<int> half(N);
+  k_rowlens<<<S->nblk, kBlock, 0, S->stream>>>(N, S->iperm, S->row_len, S->row_lo, S->liq);
+  S->launches++;
+  CK(cudaMemcpyAsync(half.data(), S->liq, sizeof(int) * N, cudaMemcpyDeviceToHost,
                      S->stream));
-  CK(cudaMemcpyAsync(lo.data(), S->row_lo, sizeof(int) * N, cudaMemcpyDeviceToHost, S->stream));
   CK(cudaStreamSynchronize(S->stream));
   std::vector<long long> hs(N);
   long long tot = 0;
   for (int i = 0; i < N; i++) {
     hs[i] = tot;
-    tot += 1 + (len[i] - lo[i]);
+    tot += 1 + half[i];
   }
   if (nentries) *nentries = tot;
   if (atnidx)
@@ -573,8 +537,8 @@ extern "C" int clmd_get_halflist(clmd_system* S, int32_t* atnlist, int64_t cap,
     CK(cudaMalloc(&dout, sizeof(int) * (tot + 1)));
     CK(cudaMemcpyAsync(dhs, hs.data(), sizeof(long long) * N, cudaMemcpyHostToDevice,
                        S->stream));
-    k_halflist<<<S->nblk, kBlock, 0, S->stream>>>(N, S->list, S->row_start, S->row_len,
-                                                   S->row_lo, dhs, dout);
+    k_halflist<<<S->nblk, kBlock, 0, S->stream>>>(N, S->iperm, S->perm, S->list, S->row_start,
+                                                   S->row_len, S->row_lo, dhs, dout);
     S->launches++;
     CK(cudaMemcpyAsync(atnlist, dout, sizeof(int) * tot, cudaMemcpyDeviceToHost, S->stream));
     CK(cudaStreamSynchronize(S->stream));
@@ -582,11 +546,6 @@ extern "C" int clmd_get_halflist(clmd_system* S, int32_t* atnlist, int64_t cap,
     cudaFree(dout);
   }
   return set_last(CLMD_OK);
-}
-
-__global__ void k_plus1(int n, const int* in, int* out) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) out[i] = in[i];
 }
 
 extern "C" int clmd_get_clusters(clmd_system* S, const clmd_cluster_view* v) {

@@ -17,27 +17,30 @@
 
 namespace clmd {
 
+// Union-find over storage slots keyed by the reference index key[] (slot ->
+// atom number): a root is linked under the root with the smaller key, so a
+// component's root is its atom with the smallest reference index.
 __device__ __forceinline__ int uf_find(int* par, int x) {
   for (;;) {
     int p = __ldcg(par + x);
     if (p == x) return x;
     int gp = __ldcg(par + p);
-    if (gp != p) par[x] = gp;  // halving; parents only ever decrease
+    if (gp != p) par[x] = gp;  // halving; keys only ever decrease along a path
     x = gp;
   }
 }
 
-__device__ __forceinline__ void uf_union(int* par, int a, int b) {
+__device__ __forceinline__ void uf_union(int* par, const int* key, int a, int b) {
   for (;;) {
     a = uf_find(par, a);
     b = uf_find(par, b);
     if (a == b) return;
-    if (a < b) {
+    if (key[a] < key[b]) {
       int t = a;
       a = b;
       b = t;
     }
-    int old = atomicCAS(par + a, a, b);
+    int old = atomicCAS(par + a, a, b);  // a has the larger key
     if (old == a) return;
   }
 }
@@ -99,13 +102,14 @@ __global__ void k_clu_init(Params P, DevState* st, int* parent, int* cs, double*
 // ascending).  Stillinger: species-1 atoms only, and a species-2 neighbour
 // ends the row (:85).  tWF: every pair, with degree counts for the liquid
 // test and the bond kept for the second (liquid-only) union-find.
-__global__ void k_clu_bonds(Params P, DevState* st, const double4* pos, const int* list,
-                            const int* row_start, const int* row_len, const int* row_lo,
-                            int* parent, int* deg, int* deg1, int2* bonds,
+__global__ void k_clu_bonds(Params P, DevState* st, const double4* pos, const int* perm,
+                            const int* list, const int* row_start, const int* row_len,
+                            const int* row_lo, int* parent, int* deg, int* deg1, int2* bonds,
                             unsigned long long* nbonds, int bond_cap) {
   if (clu_gate(st)) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= P.N - 1) return;  // the last atom has no row (:74)
+  if (i >= P.N) return;
+  if (perm[i] == P.N - 1) return;  // the last atom has no row (:74)
   bool fre = P.clustering == CLMD_CLU_FRENKEL;
   double4 pi = pos[i];
   int si = (int)pi.w;
@@ -123,7 +127,7 @@ __global__ void k_clu_bonds(Params P, DevState* st, const double4* pos, const in
     double dz = mimage_bf(pi.z - pj.z, P.boxz, P.ibz, bf1, bf2);
     double rij2 = dx * dx + dy * dy + dz * dz;
     if (rij2 <= P.atskin2) {
-      uf_union(parent, i, j);
+      uf_union(parent, perm, i, j);
       if (fre) {
         atomicAdd(deg + i, 1);
         atomicAdd(deg + j, 1);
@@ -139,14 +143,14 @@ __global__ void k_clu_bonds(Params P, DevState* st, const double4* pos, const in
 
 // labels (1-based, = smallest atom index of the component), sizes and
 // kinetic energy per label
-__global__ void k_clu_label(Params P, DevState* st, const double4* pos, const double* vx,
-                            const double* vy, const double* vz, int* parent, int* cl, int* cs,
-                            double* cek, int* cgs) {
+__global__ void k_clu_label(Params P, DevState* st, const double4* pos, const int* perm,
+                            const double* vx, const double* vy, const double* vz, int* parent,
+                            int* cl, int* cs, double* cek, int* cgs) {
   if (clu_gate(st)) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P.N) return;
-  int r = uf_find(parent, i);
-  cl[i] = r + 1;
+  int r = perm[uf_find(parent, i)];
+  cl[perm[i]] = r + 1;
   int sp = (int)pos[i].w;
   bool fre = P.clustering == CLMD_CLU_FRENKEL;
   if (fre && sp != 1) {
@@ -160,33 +164,39 @@ __global__ void k_clu_label(Params P, DevState* st, const double4* pos, const do
 // stoddard-pbc-n-m.f:152-155 / -fre.f:229-234: one histogram entry per label
 // value 1..natom (labels that are not a root have cs = 0 and land in csi(0),
 // which the reference never resets)
+constexpr int kSmallBins = 64;
+
 __global__ void k_clu_hist(Params P, DevState* st, const int* cs, const double* cek, int* csi,
-                           double* ceks, int* cgsa, const int* cgs) {
+                           double* ceks) {
   if (clu_gate(st)) return;
-  __shared__ int zero_cnt;
+  __shared__ int hc[kSmallBins];
+  __shared__ double he[kSmallBins];
   __shared__ int bmax;
-  if (threadIdx.x == 0) {
-    zero_cnt = 0;
-    bmax = 0;
+  for (int b = threadIdx.x; b < kSmallBins; b += blockDim.x) {
+    hc[b] = 0;
+    he[b] = 0.0;
   }
+  if (threadIdx.x == 0) bmax = 0;
   __syncthreads();
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k < P.N) {
     int s = cs[k];
-    if (s == 0) {
-      atomicAdd(&zero_cnt, 1);
-      if (cek[k] != 0.0) atomicAdd(ceks, cek[k]);
+    double e = cek[k];
+    if (s < kSmallBins) {
+      atomicAdd(&hc[s], 1);
+      if (e != 0.0) atomicAdd(&he[s], e);
     } else {
       atomicAdd(csi + s, 1);
-      atomicAdd(ceks + s, cek[k]);
-      atomicMax(&bmax, s);
+      atomicAdd(ceks + s, e);
     }
+    if (s > 0) atomicMax(&bmax, s);
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    if (zero_cnt) atomicAdd(csi, zero_cnt);
-    atomicMax(&st->s.maxcs, bmax);
+  for (int b = threadIdx.x; b < kSmallBins; b += blockDim.x) {
+    if (hc[b]) atomicAdd(csi + b, hc[b]);
+    if (he[b] != 0.0) atomicAdd(ceks + b, he[b]);
   }
+  if (threadIdx.x == 0 && bmax > 0) atomicMax(&st->s.maxcs, bmax);
 }
 
 __global__ void k_clu_prep(DevState* st) {
@@ -213,9 +223,10 @@ __global__ void k_clu_finish(Params P, DevState* st, int* cfpt) {
 
 // liquid atoms and cekf(0) (species-1 atoms with >= atnenum bonds of which
 // fewer than atnenum go to species 1)
-__global__ void k_liq_flag(Params P, DevState* st, const double4* pos, const double* vx,
-                           const double* vy, const double* vz, const int* deg,
-                           const int* deg1, int* liq, int* parent2, double* cekf) {
+__global__ void k_liq_flag(Params P, DevState* st, const double4* pos, const int* perm,
+                           const double* vx, const double* vy, const double* vz,
+                           const int* deg, const int* deg1, int* liq, int* liqref,
+                           int* parent2, double* cekf) {
   if (clu_gate(st)) return;
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= P.N) return;
@@ -228,6 +239,7 @@ __global__ void k_liq_flag(Params P, DevState* st, const double4* pos, const dou
       atomicAdd(cekf, kin_energy(P, sp, vx[k], vy[k], vz[k]));
   }
   liq[k] = l;
+  liqref[perm[k]] = l;
   parent2[k] = k;
 }
 
@@ -296,33 +308,34 @@ __global__ void k_liq_rank(Params P, DevState* st, const int* liq, const int* au
 }
 
 __global__ void k_liq_union(DevState* st, const int2* bonds, const unsigned long long* nbonds,
-                            int bond_cap, const int* liq, int* parent2) {
+                            int bond_cap, const int* liq, const int* perm, int* parent2) {
   if (clu_gate(st)) return;
   unsigned long long nb = *nbonds;
   if (nb > (unsigned long long)bond_cap) nb = bond_cap;
   for (unsigned long long b = blockIdx.x * blockDim.x + threadIdx.x; b < nb;
        b += (unsigned long long)gridDim.x * blockDim.x) {
     int2 e = bonds[b];
-    if (liq[e.x] && liq[e.y]) uf_union(parent2, e.x, e.y);
+    if (liq[e.x] && liq[e.y]) uf_union(parent2, perm, e.x, e.y);
   }
 }
 
 // tWF labels are the rank (1-based) of the component's smallest liquid atom
 // in liqmon(); the reference leaves clf() of non-liquid atoms as whatever
 // the flood fill wrote (:215-218), the engine writes 0 there.
-__global__ void k_liq_label(Params P, DevState* st, const double4* pos, const double* vx,
-                            const double* vy, const double* vz, const int* liq,
-                            const int* rank, int* parent2, int* clf, int* csf, double* cekf) {
+__global__ void k_liq_label(Params P, DevState* st, const double4* pos, const int* perm,
+                            const double* vx, const double* vy, const double* vz,
+                            const int* liq, const int* rank, int* parent2, int* clf, int* csf,
+                            double* cekf) {
   if (clu_gate(st)) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P.N) return;
   if (!liq[i]) {
-    clf[i] = 0;
+    clf[perm[i]] = 0;
     return;
   }
-  int r = uf_find(parent2, i);
+  int r = perm[uf_find(parent2, i)];
   int lab = rank[r] + 1;
-  clf[i] = lab;
+  clf[perm[i]] = lab;
   atomicAdd(csf + lab, 1);
   int sp = (int)pos[i].w;
   atomicAdd(cekf + lab, kin_energy(P, sp, vx[i], vy[i], vz[i]));
@@ -411,24 +424,24 @@ void stoddard_launch(clmd_system* S, int force) {
   k_clu_init<<<nb, kBlock, 0, s>>>(P, S->st, S->parent, S->cs, S->cek, S->csi, S->ceks,
                                     S->deg, S->deg1, S->cgs, S->clf, S->csf, S->csif, S->cekf,
                                     S->ceksf, S->cgsf, S->cgsa, S->cgsfa, S->nbonds);
-  k_clu_bonds<<<nb, kBlock, 0, s>>>(P, S->st, S->pos, S->list, S->row_start, S->row_len,
-                                     S->row_lo, S->parent, S->deg, S->deg1, S->bonds,
-                                     S->nbonds, S->bond_cap);
-  k_clu_label<<<nb, kBlock, 0, s>>>(P, S->st, S->pos, S->vx, S->vy, S->vz, S->parent, S->cl,
-                                     S->cs, S->cek, S->cgs);
-  k_clu_hist<<<nb, kBlock, 0, s>>>(P, S->st, S->cs, S->cek, S->csi, S->ceks, S->cgsa, S->cgs);
+  k_clu_bonds<<<nb, kBlock, 0, s>>>(P, S->st, S->pos, S->perm, S->list, S->row_start,
+                                     S->row_len, S->row_lo, S->parent, S->deg, S->deg1,
+                                     S->bonds, S->nbonds, S->bond_cap);
+  k_clu_label<<<nb, kBlock, 0, s>>>(P, S->st, S->pos, S->perm, S->vx, S->vy, S->vz, S->parent,
+                                     S->cl, S->cs, S->cek, S->cgs);
+  k_clu_hist<<<nb, kBlock, 0, s>>>(P, S->st, S->cs, S->cek, S->csi, S->ceks);
   k_clu_finish<<<1, 1, 0, s>>>(P, S->st, S->cfpt);
   S->launches += 6;
   if (P.clustering == CLMD_CLU_FRENKEL) {
-    k_liq_flag<<<nb, kBlock, 0, s>>>(P, S->st, S->pos, S->vx, S->vy, S->vz, S->deg, S->deg1,
-                                      S->liq, S->parent2, S->cekf);
-    k_liq_tiles<<<nb, kBlock, 0, s>>>(P, S->st, S->liq, S->scan_aux);
+    k_liq_flag<<<nb, kBlock, 0, s>>>(P, S->st, S->pos, S->perm, S->vx, S->vy, S->vz, S->deg,
+                                      S->deg1, S->liq, S->liqref, S->parent2, S->cekf);
+    k_liq_tiles<<<nb, kBlock, 0, s>>>(P, S->st, S->liqref, S->scan_aux);
     k_liq_top<<<1, 1024, 0, s>>>(S->st, S->scan_aux, nb);
-    k_liq_rank<<<nb, kBlock, 0, s>>>(P, S->st, S->liq, S->scan_aux, S->liqrank);
+    k_liq_rank<<<nb, kBlock, 0, s>>>(P, S->st, S->liqref, S->scan_aux, S->liqrank);
     int ub = 4 * S->num_sms;
     k_liq_union<<<ub, kBlock, 0, s>>>(S->st, S->bonds, S->nbonds, S->bond_cap, S->liq,
-                                       S->parent2);
-    k_liq_label<<<nb, kBlock, 0, s>>>(P, S->st, S->pos, S->vx, S->vy, S->vz, S->liq,
+                                       S->perm, S->parent2);
+    k_liq_label<<<nb, kBlock, 0, s>>>(P, S->st, S->pos, S->perm, S->vx, S->vy, S->vz, S->liq,
                                        S->liqrank, S->parent2, S->clf, S->csf, S->cekf);
     k_liq_hist<<<nb, kBlock, 0, s>>>(P, S->st, S->csf, S->cekf, S->cgsf, S->csif, S->ceksf,
                                       S->cgsfa);

@@ -17,9 +17,16 @@ struct clmd_system {
   cudaStream_t side = nullptr;  // body capture of conditional nodes
   // per-atom state
   double4* pos = nullptr;
+  double4* pos_alt = nullptr;  // second position buffer of the fused steps
   double *vx = nullptr, *vy = nullptr, *vz = nullptr;
   double *ax = nullptr, *ay = nullptr, *az = nullptr;
-  int* api = nullptr;
+  int* api = nullptr;                 // species by reference index (staging)
+  int *perm = nullptr, *iperm = nullptr;  // slot -> reference index, inverse
+  // reorder scratch (a rebuild gathers the state into cell order here)
+  double4* pos_s = nullptr;
+  double *vx_s = nullptr, *vy_s = nullptr, *vz_s = nullptr;
+  double *ax_s = nullptr, *ay_s = nullptr, *az_s = nullptr;
+  int* perm_s = nullptr;
   double *sx = nullptr, *sy = nullptr, *sz = nullptr;     // staging / scratch
   double *vxn = nullptr, *vyn = nullptr, *vzn = nullptr;  // Nose-Hoover iterate
   // neighbour list
@@ -27,11 +34,11 @@ struct clmd_system {
   int *row_start = nullptr, *row_len = nullptr, *row_lo = nullptr;
   int *cell_count = nullptr, *cell_start = nullptr, *cell_fill = nullptr;
   int *cell_atoms = nullptr, *atom_cell = nullptr;
-  double4* spos = nullptr;
   int* scan_aux = nullptr;
   int ncell_alloc = 0;
   // reductions / scalars
   double* partials = nullptr;
+  double* red = nullptr;     // partial sums of the persistent kernel
   clmd::DevState* st = nullptr;
   clmd_scalars* h_sc = nullptr;  // pinned
   // cluster analysis
@@ -41,18 +48,17 @@ struct clmd_system {
   int *cgs = nullptr, *cgsf = nullptr, *cgsa = nullptr, *cgsfa = nullptr, *cfpt = nullptr,
       *cfptf = nullptr;
   double *cek = nullptr, *cekf = nullptr, *ceks = nullptr, *ceksf = nullptr;
-  int *deg = nullptr, *deg1 = nullptr, *liq = nullptr, *liqrank = nullptr;
+  int *deg = nullptr, *deg1 = nullptr, *liq = nullptr, *liqrank = nullptr, *liqref = nullptr;
   int2* bonds = nullptr;
   unsigned long long* nbonds = nullptr;
   int bond_cap = 0;
   // launch geometry
   int nblk = 1;          // ceil(N / kBlock)
-  int coop_blocks = 1;   // co-resident blocks of the cooperative solve
+  int cyc_blocks = 1;    // co-resident blocks of the persistent kernel
   long long launches = 0;
-  // captured main-loop graphs
-  cudaGraphExec_t cyc_exec = nullptr;   // ftcsi steps, analysis first
-  cudaGraphExec_t step_exec = nullptr;  // one plain step
-  long long cyc_kernels = 0, step_kernels = 0;
+  // captured main-loop graph: analysis + ftcsi steps
+  cudaGraphExec_t cyc_exec = nullptr;
+  long long cyc_kernels = 0;
   bool graphs_ok = false;
 };
 
@@ -62,18 +68,21 @@ int check(cudaError_t e, const char* what);
 
 // clmd_md.cu
 void k_set_step_launch(clmd_system* S, int step);
-void k_step_advance_launch(clmd_system* S);
-void nb_prologue_launch(clmd_system* S);
-void rebuild_launch(clmd_system* S, cudaStream_t s);
-void drift_launch(clmd_system* S, unsigned long long cond, int use_cond);
-void force_launch(clmd_system* S, int mode);
-void nh_solve_launch(clmd_system* S);
+void clear_cells(clmd_system* S);
+void force_launch(clmd_system* S, int mode, int advance = 0);
 void thermostat_launch(clmd_system* S, int step);
 void stopdead_launch(clmd_system* S, int step);
 void zero_acc_launch(clmd_system* S);
-void pack_pos_launch(clmd_system* S, int have_x, int have_y, int have_z);
-void unpack_pos_launch(clmd_system* S);
-int coop_blocks_for(clmd_system* S);
+// host I/O through the slot permutation: staging arrays (reference order)
+// <-> state (slot order)
+void scatter_in_launch(clmd_system* S, int hx, int hy, int hz, int hvx, int hvy, int hvz,
+                       int hax, int hay, int haz);
+void gather_out_launch(clmd_system* S);
+
+// clmd_cycle.cu: the persistent step kernel (mode 0: nsteps integrator
+// steps; mode 1: one neighbor() rebuild)
+int cycle_blocks_for(clmd_system* S);
+void cycle_launch(clmd_system* S, int nsteps, int mode);
 
 // clmd_cluster.cu
 void stoddard_launch(clmd_system* S, int force);
