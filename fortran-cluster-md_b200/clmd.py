@@ -196,6 +196,8 @@ def load(path: str = LIB_PATH):
         "clmd_stoddard": ([P, C.c_int32], C.c_int),
         "clmd_chk_nucleation": ([P, i], C.c_int),
         "clmd_run": ([P, C.c_int32, C.c_int32, i], C.c_int),
+        "clmd_steps": ([P, C.c_int32, C.c_int32], C.c_int),
+        "clmd_set_device": ([C.c_int], C.c_int),
         "clmd_get_halflist": ([P, i, C.c_int64, i, C.POINTER(C.c_int64)], C.c_int),
         "clmd_get_clusters": ([P, C.POINTER(ClusterView)], C.c_int),
         "clmd_synchronize": ([P], C.c_int),
@@ -214,6 +216,12 @@ def load(path: str = LIB_PATH):
         f.restype = res
     _lib = lib
     return lib
+
+
+def set_device(dev: int):
+    st = load().clmd_set_device(dev)
+    if st:
+        raise ClmdError(st, "clmd_set_device")
 
 
 def status_string(code: int) -> str:
@@ -408,6 +416,10 @@ class System:
         nxt = C.c_int32(0)
         st = self._chk(self.lib.clmd_run(self.h, first, nsteps, C.byref(nxt)), "run")
         return st, nxt.value
+
+    def steps(self, first, nsteps):
+        """nsteps integrator() calls in one launch of the step kernel."""
+        return self._chk(self.lib.clmd_steps(self.h, first, nsteps), "steps")
 
     def synchronize(self):
         return self._chk(self.lib.clmd_synchronize(self.h), "synchronize")

@@ -402,6 +402,18 @@ extern "C" int clmd_integrator(clmd_system* S, int32_t step) {
   return fetch(S);
 }
 
+extern "C" int clmd_steps(clmd_system* S, int32_t first, int32_t nsteps) {
+  if (!S || nsteps < 0) return set_last(CLMD_ERR_ARG);
+  k_set_step_launch(S, first);
+  if (nsteps > 0) cycle_launch(S, nsteps, 0);
+  return fetch(S);
+}
+
+extern "C" int clmd_set_device(int device) {
+  CK(cudaSetDevice(device));
+  return set_last(CLMD_OK);
+}
+
 extern "C" int clmd_thermostat(clmd_system* S, int32_t step) {
   if (!S) return set_last(CLMD_ERR_ARG);
   thermostat_launch(S, step);

@@ -187,6 +187,14 @@ int clmd_get_halflist(clmd_system* sys, int32_t* atnlist, int64_t cap,
                       int32_t* atnidx, int64_t* nentries);
 int clmd_get_clusters(clmd_system* sys, const clmd_cluster_view* view);
 
+/* nsteps consecutive integrator() calls (steps first..first+nsteps-1) in
+ * one launch of the step kernel, without the main loop's analysis. */
+int clmd_steps(clmd_system* sys, int32_t first, int32_t nsteps);
+
+/* Selects the CUDA device later clmd_create calls of this thread use
+ * (a host that links another CUDA runtime cannot select it for us). */
+int clmd_set_device(int device);
+
 /* Waits for the system's stream. */
 int clmd_synchronize(clmd_system* sys);
 /* Enqueue-only timing helpers: the CUDA stream the system launches on. */
