@@ -212,6 +212,27 @@ int clmd_init_random(int32_t n, double boxx, double boxy, double boxz, double rm
                      double kT_over_m, uint64_t seed, double* x, double* y, double* z,
                      double* vx, double* vy, double* vz);
 
+/* No counterpart in the reference: the Stillinger analysis (what stoddard()
+ * of stoddard-pbc-n-m.f computes: labels cl, sizes cs, histogram csi) for
+ * callers that cannot let the library allocate device memory -- hosts that
+ * pass only buffers from their own pool or fixed budget.  It allocates
+ * nothing: its one scratch array (the union-find parents) is a file-scope
+ * device array of CLMD_NOALLOC_MAX_ATOMS ints (4 MiB) that every GPU which
+ * loads the library holds until exit.  All pointers are device pointers:
+ * x, y, z, api (1-based species), the reference's half list atnlist (nlist
+ * entries) and atnidx, and the outputs cl[natom], cs[natom],
+ * csi[natom+1] (csi[0] accumulates across calls like the reference's).
+ * Enqueued on `stream`; natom > CLMD_NOALLOC_MAX_ATOMS returns CLMD_ERR_ARG.
+ * The first call on each device looks up the array's device address (make
+ * it before any stream capture).  Every call shares the array, so calls that
+ * overlap on the GPU race: serialise them. */
+#define CLMD_NOALLOC_MAX_ATOMS (1 << 20)
+int clmd_stoddard_noalloc(int32_t natom, const double* x, const double* y, const double* z,
+                          const int32_t* api, const int32_t* atnlist, int64_t nlist,
+                          const int32_t* atnidx, double boxx, double boxy, double boxz,
+                          double atrskin, double sigma1, double atskin, int32_t* cl,
+                          int32_t* cs, int32_t* csi, void* stream);
+
 const char* clmd_status_string(int status);
 /* sizeof of the ABI structs (0 config, 1 scalars, 2 cluster view), so that
  * bindings in other languages can check their layout. */
