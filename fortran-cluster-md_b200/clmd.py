@@ -145,6 +145,38 @@ class ClusterView(C.Structure):
     ]
 
 
+class EnsConfig(C.Structure):
+    """clmd_ens_config (include/clmd.h)."""
+
+    _fields_ = [
+        ("rc", C.c_double), ("rskin", C.c_double), ("atskin", C.c_double), ("dt", C.c_double),
+        ("max_atoms", C.c_int64), ("max_replicas", C.c_int32), ("list_stride", C.c_int32),
+        ("precision", C.c_int32), ("integrator", C.c_int32), ("ftcsi", C.c_int32),
+        ("nbtim", C.c_int32), ("threads", C.c_int32), ("pad", C.c_int32),
+    ]
+
+
+class ReplicaSpec(C.Structure):
+    """clmd_replica_spec (include/clmd.h)."""
+
+    _fields_ = [
+        ("box", C.c_double), ("temp", C.c_double), ("Q", C.c_double), ("natom", C.c_int32),
+        ("csover", C.c_int32), ("clwait", C.c_int32), ("budget", C.c_int32),
+        ("ethst", C.c_char), ("pad", C.c_char * 7),
+    ]
+
+
+class ReplicaResult(C.Structure):
+    """clmd_replica_result (include/clmd.h)."""
+
+    _fields_ = [
+        ("ekin", C.c_double), ("epot", C.c_double), ("psi", C.c_double), ("s", C.c_double),
+        ("slot", C.c_int32), ("natom", C.c_int32), ("step", C.c_int32), ("status", C.c_int32),
+        ("done", C.c_int32), ("clbrkt", C.c_int32), ("maxcs", C.c_int32),
+        ("nrebuild", C.c_int32),
+    ]
+
+
 # (name, dtype, length kind) of every cluster output: "N" or "N1" (= N+1)
 CLUSTER_FIELDS = [
     ("cl", np.int32, "N"), ("cs", np.int32, "N"), ("csi", np.int32, "N1"),
@@ -209,6 +241,16 @@ def load(path: str = LIB_PATH):
         "clmd_last_status": ([], C.c_int32),
         "clmd_struct_size": ([C.c_int], C.c_int64),
         "clmd_scalars_init": ([C.POINTER(Config), C.POINTER(Scalars)], None),
+        "clmd_ens_create": ([C.POINTER(EnsConfig), C.POINTER(P)], C.c_int),
+        "clmd_ens_destroy": ([P], C.c_int),
+        "clmd_ens_add": ([P, C.POINTER(ReplicaSpec), d, d, d, d, d, d, i], C.c_int),
+        "clmd_ens_step": ([P, C.c_int32], C.c_int),
+        "clmd_ens_results": ([P, C.POINTER(ReplicaResult), C.c_int32, i], C.c_int),
+        "clmd_ens_remove": ([P, C.c_int32], C.c_int),
+        "clmd_ens_get_state": ([P, C.c_int32, d, d, d, d, d, d, d, d, d, i], C.c_int),
+        "clmd_ens_fpt": ([P, C.c_int32, i, C.c_int32], C.c_int),
+        "clmd_ens_free_atoms": ([P], C.c_int64),
+        "clmd_ens_launches": ([P], C.c_int64),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -450,3 +492,99 @@ class System:
             setattr(v, name, ptr(a, C.c_int32 if dt == np.int32 else C.c_double))
         self._chk(self.lib.clmd_get_clusters(self.h, C.byref(v)), "clusters")
         return out
+
+
+def ens_config(max_atoms, max_replicas, *, precision=PREC_MIXED, integrator=INT_NOSE, ftcsi=100,
+               rc=2.5, rskin=2.8, atskin=1.5, dt=0.005, nbtim=10, list_stride=0, threads=0):
+    c = EnsConfig()
+    c.rc, c.rskin, c.atskin, c.dt = rc, rskin, atskin, dt
+    c.max_atoms, c.max_replicas = max_atoms, max_replicas
+    c.list_stride, c.precision, c.integrator = list_stride, precision, integrator
+    c.ftcsi, c.nbtim, c.threads = ftcsi, nbtim, threads
+    return c
+
+
+class Ensemble:
+    """Independent replicas advanced together (clmd_ensemble*)."""
+
+    def __init__(self, cfg: EnsConfig):
+        self.lib = load()
+        self.cfg = cfg
+        h = C.c_void_p()
+        st = self.lib.clmd_ens_create(C.byref(cfg), C.byref(h))
+        if st:
+            raise ClmdError(st, "clmd_ens_create")
+        self.h = h
+        self.natom = {}
+
+    def close(self):
+        if self.h:
+            self.lib.clmd_ens_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, natom, box, temp, x, y, z, vx, vy, vz, *, csover=0, clwait=0, budget=0,
+            ethst="N", q=0.0):
+        """Admits a replica; returns its slot, or None if there is no room."""
+        sp = ReplicaSpec()
+        sp.natom, sp.box, sp.temp, sp.Q = natom, box, temp, q
+        sp.csover, sp.clwait, sp.budget = csover, clwait, budget
+        sp.ethst = ethst.encode()
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z, vx, vy, vz)]
+        slot = C.c_int32(-1)
+        st = self.lib.clmd_ens_add(self.h, C.byref(sp), *[ptr(a, C.c_double) for a in arrs],
+                                   C.byref(slot))
+        if st == ERR_NOMEM:
+            return None
+        if st:
+            raise ClmdError(st, "clmd_ens_add")
+        self.natom[slot.value] = natom
+        return slot.value
+
+    def step(self, nwin=1):
+        st = self.lib.clmd_ens_step(self.h, nwin)
+        if st:
+            raise ClmdError(st, "clmd_ens_step")
+
+    def results(self):
+        cap = len(self.natom) + 1
+        out = (ReplicaResult * cap)()
+        n = C.c_int32(0)
+        st = self.lib.clmd_ens_results(self.h, out, cap, C.byref(n))
+        if st:
+            raise ClmdError(st, "clmd_ens_results")
+        return {out[k].slot: out[k] for k in range(n.value)}
+
+    def remove(self, slot):
+        st = self.lib.clmd_ens_remove(self.h, slot)
+        if st:
+            raise ClmdError(st, "clmd_ens_remove")
+        self.natom.pop(slot, None)
+
+    def state(self, slot):
+        n = self.natom[slot]
+        arrs = [np.zeros(n) for _ in range(9)]
+        cl = np.zeros(n, dtype=np.int32)
+        st = self.lib.clmd_ens_get_state(self.h, slot, *[ptr(a, C.c_double) for a in arrs],
+                                         ptr(cl, C.c_int32))
+        if st:
+            raise ClmdError(st, "clmd_ens_get_state")
+        return State(*arrs), cl
+
+    def fpt(self, slot, cap=128):
+        a = np.zeros(cap, dtype=np.int32)
+        st = self.lib.clmd_ens_fpt(self.h, slot, ptr(a, C.c_int32), cap)
+        if st:
+            raise ClmdError(st, "clmd_ens_fpt")
+        return a
+
+    def free_atoms(self):
+        return self.lib.clmd_ens_free_atoms(self.h)
+
+    def launches(self):
+        return self.lib.clmd_ens_launches(self.h)

@@ -1,0 +1,1206 @@
+// clmd_ensemble.cu -- batched / served ensembles of independent replicas.
+//
+// One persistent launch per window: each CTA repeatedly claims a replica
+// (largest first) from a device counter and runs it through one window --
+// the Stillinger analysis + chk_nucleation at the window's first step, then
+// ftcsi integrator steps -- with every phase separated by __syncthreads
+// instead of a grid barrier.  The replica's positions (FP64) stay in shared
+// memory for the whole window when they fit (<= ~8k atoms per CTA), so the
+// neighbour gathers of the list search, the forces and the cluster test never
+// leave the SM.  Per replica the algorithm is the drop-in's: adaptive-skin
+// Verlet list (neighbor-pbc-mav.f) on a counting-sorted cell grid, velocity
+// Verlet (int-verlet-mav.f) or Nose-Hoover (int-verlet-nh-mav.f), the
+// Stillinger criterion (stoddard-pbc-n-m.f) and chk_nucleation
+// (chk-nucleation.f); the start sequence (stopdead-m.f, neighbor(0),
+// AccAtom, main.f:156-166) runs on the device when a replica is admitted.
+//
+// Mixed precision: minimum image, cut-off test, list and cluster tests in
+// FP64 on FP64 positions; each pair term (1/r^2, r^-6, f_ij and its
+// components) in FP32, summed per atom in FP32 with Kahan compensation in a
+// fixed order (rows ordered by the cell sweep over index-sorted cells), so a
+// replica's result does not depend on which other replicas share the launch.
+// Positions, velocities, PSI, energies and the virial stay FP64.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <mutex>
+#include <vector>
+
+#include "../../include/clmd.h"
+
+namespace clmd_ens {
+
+constexpr int kFptCap = 128;  // first-passage sizes tracked per replica
+constexpr int kNcMax = 20;    // cells per dimension at most (cells never narrower than the list radius)
+
+struct Rep {
+  // parameters (reduced units: sigma = eps = m = 1)
+  double box, ibox, att, Q, nkt3_i, nkt3_d, ekinT;
+  int natom, off, csover, clwait, budget;
+  int ethst;
+  // state
+  double psi, s, sumv2, ekin, epot, virial;
+  double atrskin, dmms, dmmsu, dmmax, dmmav;
+  double dmmh[256];
+  int dmmst, dmmi, step, status, done, clbrkt, maxcs, fpt_top, nrebuild, cstep, started;
+  int pad;
+};
+
+struct Args {
+  double *x, *y, *z, *vx, *vy, *vz;
+  double *vxn, *vyn, *vzn;
+  void* a;  // float[3][pool] (mixed) or double[3][pool] (FP64)
+  long long pool;
+  int *list, *rlen, *sorted, *cellid, *parent, *cs, *cl, *fpt;
+  Rep* reps;
+  const int* items;
+  int nitems;
+  int* ctr;
+  double rc, atskin, dt;
+  int nbtim, ftcsi, lstride, integrator, nwin;
+  int ncmax;  // cells per dimension this launch's shared memory holds
+  int4* summary;  // per slot: done, status, step, maxcs
+};
+
+__device__ __forceinline__ double wsum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double wmax(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// block-wide sum returned to every thread, fixed shape: deterministic
+template <int NT>
+__device__ __forceinline__ double cta_sum(double v, double* sh) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  v = wsum(v);
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    double t = lane < NT / 32 ? sh[lane] : 0.0;
+    t = wsum(t);
+    if (lane == 0) sh[32] = t;
+  }
+  __syncthreads();
+  double r = sh[32];
+  __syncthreads();
+  return r;
+}
+template <int NT>
+__device__ __forceinline__ double cta_max(double v, double* sh) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  v = wmax(v);
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    double t = lane < NT / 32 ? sh[lane] : 0.0;
+    t = wmax(t);
+    if (lane == 0) sh[32] = t;
+  }
+  __syncthreads();
+  double r = sh[32];
+  __syncthreads();
+  return r;
+}
+
+__device__ __forceinline__ void kahan(float& s, float& c, float t) {
+  float y = __fsub_rn(t, c);
+  float u = __fadd_rn(s, y);
+  c = __fsub_rn(__fsub_rn(u, s), y);
+  s = u;
+}
+
+// the reference's minimum images (neighbor-pbc-mav.f:84, for-a-lj-n-pbc-m.f:109)
+__device__ __forceinline__ double mi_nb(double d, double L, double iL) {
+  return __dsub_rn(__dadd_rn(d, L), __dmul_rn(L, (double)(int)__dadd_rn(1.5, __dmul_rn(d, iL))));
+}
+__device__ __forceinline__ double mi_bf(double d, double L, double iL, double bf1, double bf2) {
+  return __dadd_rn(d, __dmul_rn(L, __dsub_rn(bf1, (double)(int)__dadd_rn(bf2, __dmul_rn(d, iL)))));
+}
+
+struct Cta {
+  double* sx;  // positions in shared memory (nullptr: global)
+  double* sy;
+  double* sz;
+  int* cstart;  // [ncell + 1]
+  int* cfill;   // [ncell]
+  double red[40];
+  int ncx, ncell, nox, offx[3];
+  double cf, rs2;
+  int flag;
+  int rep;  // slot of the replica being run
+};
+
+template <bool SM>
+struct Pos {
+  const Args& A;
+  const Cta& C;
+  int off;
+  __device__ __forceinline__ double x(int i) const { return SM ? C.sx[i] : A.x[off + i]; }
+  __device__ __forceinline__ double y(int i) const { return SM ? C.sy[i] : A.y[off + i]; }
+  __device__ __forceinline__ double z(int i) const { return SM ? C.sz[i] : A.z[off + i]; }
+  __device__ __forceinline__ void set(int i, double a, double b, double c) const {
+    if (SM) {
+      C.sx[i] = a; C.sy[i] = b; C.sz[i] = c;
+    } else {
+      A.x[off + i] = a; A.y[off + i] = b; A.z[off + i] = c;
+    }
+  }
+};
+
+// neighbor-pbc-mav.f:48-60, 101-105 on the replica record (thread 0)
+__device__ bool prologue(Rep& R, Cta& C, const Args& A, int step) {
+  const int kNcMax = A.ncmax;
+  if (R.dmms > (R.atrskin - A.rc)) {
+    if (R.status == 0) R.status = CLMD_ERR_SKIN;
+    return false;
+  }
+  R.dmmav = (double)(float)R.dmmst * R.dmmsu / 256.0;
+  if (step != 0 && step > 0) {
+    R.atrskin = A.rc + (R.atrskin - A.rc) * (double)A.nbtim / (double)R.dmmst;
+    R.atrskin = fmin(R.box / 2.0, R.atrskin);
+  }
+  C.rs2 = R.atrskin * R.atrskin;
+  int n = (int)floor(R.box / (R.atrskin * (1.0 + 1e-9)));
+  n = max(1, min(n, kNcMax));
+  C.ncx = n;
+  C.ncell = n * n * n;
+  C.cf = (double)n / R.box;
+  if (n >= 3) {
+    C.nox = 3; C.offx[0] = -1; C.offx[1] = 0; C.offx[2] = 1;
+  } else if (n == 2) {
+    C.nox = 2; C.offx[0] = 0; C.offx[1] = 1;
+  } else {
+    C.nox = 1; C.offx[0] = 0;
+  }
+  R.dmmax = fmax(R.dmms, R.dmmax);
+  R.dmms = 0.0;
+  R.dmmst = 0;
+  R.nrebuild++;
+  return true;
+}
+
+// cell list + rows (ELL, transposed per replica: entry k of atom i at
+// list[off*stride + k*N + i]); cells are index-sorted so row order is fixed
+template <int NT, bool SM>
+__device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
+  const int N = R.natom, off = R.off, tid = threadIdx.x;
+  const double L = R.box;
+  for (int c = tid; c < C.ncell; c += NT) C.cfill[c] = 0;
+  __syncthreads();
+  for (int i = tid; i < N; i += NT) {
+    double x = fmod(fmod(P.x(i), L) + L, L);
+    double y = fmod(fmod(P.y(i), L) + L, L);
+    double z = fmod(fmod(P.z(i), L) + L, L);
+    P.set(i, x, y, z);
+    int cx = min((int)(x * C.cf), C.ncx - 1), cy = min((int)(y * C.cf), C.ncx - 1),
+        cz = min((int)(z * C.cf), C.ncx - 1);
+    int c = (cz * C.ncx + cy) * C.ncx + cx;
+    A.cellid[off + i] = c;
+    atomicAdd(&C.cfill[c], 1);
+  }
+  __syncthreads();
+  // exclusive scan of the counts (thread 0 walks warp sums)
+  {
+    __shared__ int wsums[NT / 32 + 1];
+    const int per = (C.ncell + NT - 1) / NT;
+    int b0 = tid * per, s = 0;
+    for (int k = 0; k < per; k++)
+      if (b0 + k < C.ncell) s += C.cfill[b0 + k];
+    int lane = tid & 31, w = tid >> 5, incl = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) wsums[w] = incl;
+    __syncthreads();
+    if (tid == 0) {
+      int acc = 0;
+      for (int k = 0; k < NT / 32; k++) {
+        int t = wsums[k];
+        wsums[k] = acc;
+        acc += t;
+      }
+    }
+    __syncthreads();
+    int ex = wsums[w] + incl - s;
+    for (int k = 0; k < per; k++)
+      if (b0 + k < C.ncell) {
+        int v = C.cfill[b0 + k];
+        C.cstart[b0 + k] = ex;
+        ex += v;
+      }
+    if (tid == 0) C.cstart[C.ncell] = N;
+    __syncthreads();
+  }
+  for (int c = tid; c < C.ncell; c += NT) C.cfill[c] = C.cstart[c];
+  __syncthreads();
+  for (int i = tid; i < N; i += NT) {
+    int slot = atomicAdd(&C.cfill[A.cellid[off + i]], 1);
+    A.sorted[off + slot] = i;
+  }
+  __syncthreads();
+  // order each cell by atom index (fixed row order)
+  for (int c = tid; c < C.ncell; c += NT) {
+    int c0 = C.cstart[c], c1 = C.cstart[c + 1];
+    for (int a = c0 + 1; a < c1; a++) {
+      int key = A.sorted[off + a], b = a - 1;
+      while (b >= c0 && A.sorted[off + b] > key) {
+        A.sorted[off + b + 1] = A.sorted[off + b];
+        b--;
+      }
+      A.sorted[off + b + 1] = key;
+    }
+  }
+  __syncthreads();
+  const double iL = R.ibox, rs2 = C.rs2;
+  const long long lbase = (long long)off * A.lstride;
+  int over = 0;
+  for (int i = tid; i < N; i += NT) {
+    const double xi = P.x(i), yi = P.y(i), zi = P.z(i);
+    int cx = min((int)(xi * C.cf), C.ncx - 1), cy = min((int)(yi * C.cf), C.ncx - 1),
+        cz = min((int)(zi * C.cf), C.ncx - 1);
+    int n = 0;
+    for (int a = 0; a < C.nox; a++) {
+      int zz = cz + C.offx[a];
+      zz += zz < 0 ? C.ncx : 0;
+      zz -= zz >= C.ncx ? C.ncx : 0;
+      for (int b = 0; b < C.nox; b++) {
+        int yy = cy + C.offx[b];
+        yy += yy < 0 ? C.ncx : 0;
+        yy -= yy >= C.ncx ? C.ncx : 0;
+        for (int d = 0; d < C.nox; d++) {
+          int xx = cx + C.offx[d];
+          xx += xx < 0 ? C.ncx : 0;
+          xx -= xx >= C.ncx ? C.ncx : 0;
+          int c = (zz * C.ncx + yy) * C.ncx + xx;
+          for (int q = C.cstart[c]; q < C.cstart[c + 1]; q++) {
+            int j = A.sorted[off + q];
+            if (j == i) continue;
+            // the reference's test in its orientation (row of the smaller index)
+            double dx, dy, dz;
+            if (i < j) {
+              dx = xi - P.x(j); dy = yi - P.y(j); dz = zi - P.z(j);
+            } else {
+              dx = P.x(j) - xi; dy = P.y(j) - yi; dz = P.z(j) - zi;
+            }
+            dx = mi_nb(dx, L, iL);
+            dy = mi_nb(dy, L, iL);
+            dz = mi_nb(dz, L, iL);
+            double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+            if (r2 <= rs2) {
+              if (n < A.lstride) A.list[lbase + (long long)n * N + i] = j;
+              n++;
+            }
+          }
+        }
+      }
+    }
+    if (n > A.lstride) {
+      over = 1;
+      n = A.lstride;
+    }
+    A.rlen[off + i] = n;
+  }
+  over = __syncthreads_or(over);
+  if (over) {
+    if (tid == 0 && R.status == 0) R.status = CLMD_ERR_LIST_OVERFLOW;
+    __syncthreads();
+    return false;
+  }
+  return true;
+}
+
+// int-verlet-mav.f:64-74 skin bookkeeping (thread 0)
+__device__ int skin(Rep& R, const Args& A, double dmmr) {
+  dmmr = 2.2 * sqrt(dmmr);
+  R.dmms = R.dmms + dmmr;
+  R.dmmsu = R.dmmsu + dmmr - R.dmmh[R.dmmi];
+  R.dmmh[R.dmmi] = dmmr;
+  R.dmmi = (R.dmmi + 1) & 255;
+  R.dmmst = R.dmmst + 1;
+  return R.dmms > (R.atrskin - A.rc - 2.0 * R.dmms / (double)(float)R.dmmst);
+}
+
+// pair forces (for-a-lj-n-pbc-m.f, sigma = eps = m = 1) -> a; optional
+// velocity-Verlet second half kick; FP64 energy/virial sums when asked
+template <int NT, bool SM, bool MIXED>
+__device__ void forces(Rep& R, Cta& C, const Args& A, const Pos<SM>& P, bool kick,
+                       bool energies) {
+  const int N = R.natom, off = R.off, tid = threadIdx.x;
+  const double L = R.box, iL = R.ibox, rc2 = A.rc * A.rc, dt = A.dt;
+  const double bf1 = 2.0 + (double)(int)(R.atrskin);
+  const double bf2 = bf1 + 0.5;
+  const long long lbase = (long long)off * A.lstride;
+  double esum = 0.0, vir = 0.0, ek = 0.0;
+  for (int i = tid; i < N; i += NT) {
+    const double xi = P.x(i), yi = P.y(i), zi = P.z(i);
+    const int len = A.rlen[off + i];
+    double ax, ay, az;
+    if (MIXED) {
+      float fx = 0.f, fy = 0.f, fz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+      for (int k = 0; k < len; k++) {
+        int j = A.list[lbase + (long long)k * N + i];
+        double dx = mi_bf(xi - P.x(j), L, iL, bf1, bf2);
+        double dy = mi_bf(yi - P.y(j), L, iL, bf1, bf2);
+        double dz = mi_bf(zi - P.z(j), L, iL, bf1, bf2);
+        double r2d = dx * dx + dy * dy + dz * dz;
+        if (r2d <= rc2) {
+          float r2 = (float)r2d;
+          float ri2 = 1.0f / r2;
+          float r6 = ri2 * ri2 * ri2;
+          float fij = 48.0f * ri2 * r6 * (r6 - 0.5f);
+          kahan(fx, cx, fij * (float)dx);
+          kahan(fy, cy, fij * (float)dy);
+          kahan(fz, cz, fij * (float)dz);
+          if (energies && i < j) {
+            esum += (double)(4.0f * r6 * (r6 - 1.0f));
+            vir += (double)(fij * r2);
+          }
+        }
+      }
+      float* a = (float*)A.a;
+      a[off + i] = fx;
+      a[A.pool + off + i] = fy;
+      a[2 * A.pool + off + i] = fz;
+      ax = (double)fx;
+      ay = (double)fy;
+      az = (double)fz;
+    } else {
+      double fx = 0.0, fy = 0.0, fz = 0.0;
+      for (int k = 0; k < len; k++) {
+        int j = A.list[lbase + (long long)k * N + i];
+        double dx = mi_bf(xi - P.x(j), L, iL, bf1, bf2);
+        double dy = mi_bf(yi - P.y(j), L, iL, bf1, bf2);
+        double dz = mi_bf(zi - P.z(j), L, iL, bf1, bf2);
+        double r2d = dx * dx + dy * dy + dz * dz;
+        if (r2d <= rc2) {
+          double ri2 = 1.0 / r2d;
+          double r6 = ri2 * ri2 * ri2;
+          double fij = 48.0 * ri2 * r6 * (r6 - 0.5);
+          fx += fij * dx;
+          fy += fij * dy;
+          fz += fij * dz;
+          if (energies && i < j) {
+            esum += 4.0 * r6 * (r6 - 1.0);
+            vir += fij * r2d;
+          }
+        }
+      }
+      double* a = (double*)A.a;
+      a[off + i] = fx;
+      a[A.pool + off + i] = fy;
+      a[2 * A.pool + off + i] = fz;
+      ax = fx;
+      ay = fy;
+      az = fz;
+    }
+    if (kick) {
+      double vxi = A.vx[off + i] + 0.5 * ax * dt;
+      double vyi = A.vy[off + i] + 0.5 * ay * dt;
+      double vzi = A.vz[off + i] + 0.5 * az * dt;
+      A.vx[off + i] = vxi;
+      A.vy[off + i] = vyi;
+      A.vz[off + i] = vzi;
+      if (energies) ek += 0.5 * (vxi * vxi + vyi * vyi + vzi * vzi);
+    }
+  }
+  if (energies) {
+    double e = cta_sum<NT>(esum, C.red);
+    double w = cta_sum<NT>(vir, C.red);
+    double k = kick ? cta_sum<NT>(ek, C.red) : 0.0;
+    if (tid == 0) {
+      R.epot = e;
+      R.virial = w;
+      if (kick) R.ekin = k;
+    }
+  }
+  __syncthreads();
+}
+
+template <bool MIXED>
+__device__ __forceinline__ void get_a(const Args& A, int k, double& ax, double& ay, double& az) {
+  if (MIXED) {
+    const float* a = (const float*)A.a;
+    ax = a[k];
+    ay = a[A.pool + k];
+    az = a[2 * A.pool + k];
+  } else {
+    const double* a = (const double*)A.a;
+    ax = a[k];
+    ay = a[A.pool + k];
+    az = a[2 * A.pool + k];
+  }
+}
+
+// stopdead-m.f:28-69 (one species, m = 1): COM removal and rescale to T
+template <int NT>
+__device__ void stopdead(Rep& R, Cta& C, const Args& A) {
+  const int N = R.natom, off = R.off, tid = threadIdx.x;
+  for (int loop = 0; loop < 10; loop++) {
+    double px = 0, py = 0, pz = 0;
+    for (int i = tid; i < N; i += NT) {
+      px += A.vx[off + i];
+      py += A.vy[off + i];
+      pz += A.vz[off + i];
+    }
+    double vxs = cta_sum<NT>(px, C.red) / (double)N;
+    double vys = cta_sum<NT>(py, C.red) / (double)N;
+    double vzs = cta_sum<NT>(pz, C.red) / (double)N;
+    double ek = 0.0;
+    for (int i = tid; i < N; i += NT) {
+      double a = A.vx[off + i] - vxs, b = A.vy[off + i] - vys, c = A.vz[off + i] - vzs;
+      A.vx[off + i] = a;
+      A.vy[off + i] = b;
+      A.vz[off + i] = c;
+      ek += 0.5 * (a * a + b * b + c * c);
+    }
+    ek = cta_sum<NT>(ek, C.red);
+    double kf = sqrt(R.ekinT / ek);  // scalev-nh-m.f with step = -1
+    for (int i = tid; i < N; i += NT) {
+      A.vx[off + i] *= kf;
+      A.vy[off + i] *= kf;
+      A.vz[off + i] *= kf;
+    }
+    if (tid == 0) R.ekin = R.ekinT;
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ int ufind(int* par, int x) {
+  for (;;) {
+    int p = __ldcg(par + x);
+    if (p == x) return x;
+    int gp = __ldcg(par + p);
+    if (gp != p) par[x] = gp;
+    x = gp;
+  }
+}
+__device__ __forceinline__ void uunion(int* par, int a, int b) {
+  for (;;) {
+    a = ufind(par, a);
+    b = ufind(par, b);
+    if (a == b) return;
+    if (a < b) {
+      int t = a;
+      a = b;
+      b = t;
+    }
+    if (atomicCAS(par + a, a, b) == a) return;
+  }
+}
+
+// stoddard-pbc-n-m.f (one species) + chk-nucleation.f at step `step`
+template <int NT, bool SM>
+__device__ void analysis(Rep& R, Cta& C, const Args& A, const Pos<SM>& P, int step) {
+  const int N = R.natom, off = R.off, tid = threadIdx.x;
+  int* par = A.parent + off;
+  int* cs = A.cs + off;
+  for (int i = tid; i < N; i += NT) {
+    par[i] = i;
+    cs[i] = 0;
+  }
+  __syncthreads();
+  const double L = R.box, iL = R.ibox, rc2 = A.atskin * A.atskin;
+  const double bf1 = (double)(int)(R.atrskin) + 2.0, bf2 = bf1 + 0.5;
+  const long long lbase = (long long)off * A.lstride;
+  for (int i = tid; i < N - 1; i += NT) {
+    const double xi = P.x(i), yi = P.y(i), zi = P.z(i);
+    const int len = A.rlen[off + i];
+    for (int k = 0; k < len; k++) {
+      int j = A.list[lbase + (long long)k * N + i];
+      if (j <= i) continue;
+      double dx = mi_bf(__dsub_rn(xi, P.x(j)), L, iL, bf1, bf2);
+      double dy = mi_bf(__dsub_rn(yi, P.y(j)), L, iL, bf1, bf2);
+      double dz = mi_bf(__dsub_rn(zi, P.z(j)), L, iL, bf1, bf2);
+      double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+      if (r2 <= rc2) uunion(par, i, j);
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < N; i += NT) {
+    int r = ufind(par, i);
+    A.cl[off + i] = r + 1;
+    atomicAdd(cs + r, 1);
+  }
+  __syncthreads();
+  double m = 0.0;
+  for (int i = tid; i < N; i += NT) m = fmax(m, (double)cs[i]);
+  int maxcs = (int)cta_max<NT>(m, C.red);
+  if (tid == 0) {
+    R.maxcs = maxcs;
+    R.cstep = step;
+    // first step at which the largest cluster reached each size
+    int* fpt = A.fpt + (size_t)C.rep * kFptCap;
+    for (int s = R.fpt_top + 1; s <= maxcs && s <= kFptCap; s++) fpt[s - 1] = step;
+    if (maxcs > R.fpt_top) R.fpt_top = maxcs;
+    // chk-nucleation.f:33-56
+    int tim = (maxcs >= R.csover && R.csover <= N) ? step : 0;
+    if (tim > 0) {
+      if (R.clbrkt == 0)
+        R.clbrkt = tim;
+      else if ((tim - R.clbrkt) >= R.clwait)
+        R.done = 1;
+    } else {
+      R.clbrkt = 0;
+    }
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// one replica, one window
+// ---------------------------------------------------------------------------
+template <int NT, bool SM, bool MIXED>
+__device__ void run_window(Rep& R, Cta& C, const Args& A) {
+  const int tid = threadIdx.x;
+  const int N = R.natom, off = R.off;
+  const bool nh = A.integrator == CLMD_INT_NOSE;
+  const double dt = A.dt;
+  Pos<SM> P{A, C, off};
+  if (SM) {
+    for (int i = tid; i < N; i += NT) {
+      C.sx[i] = A.x[off + i];
+      C.sy[i] = A.y[off + i];
+      C.sz[i] = A.z[off + i];
+    }
+    __syncthreads();
+  }
+  // the grid of the current list
+  if (tid == 0) {
+    int n = (int)floor(R.box / (R.atrskin * (1.0 + 1e-9)));
+    n = max(1, min(n, A.ncmax));
+    C.ncx = n;
+    C.ncell = n * n * n;
+    C.cf = (double)n / R.box;
+    C.rs2 = R.atrskin * R.atrskin;
+    C.nox = n >= 3 ? 3 : n;
+    C.offx[0] = n >= 3 ? -1 : 0;
+    C.offx[1] = n >= 3 ? 0 : 1;
+    C.offx[2] = 1;
+  }
+  __syncthreads();
+  if (!R.started) {
+    // stopdead(-1), neighbor(0), a = 0 + AccAtom, main.f:156-166
+    stopdead<NT>(R, C, A);
+    if (tid == 0) C.flag = prologue(R, C, A, 0);
+    __syncthreads();
+    if (!C.flag || !rebuild<NT, SM>(R, C, A, P)) goto out;
+    forces<NT, SM, MIXED>(R, C, A, P, false, true);
+    if (tid == 0) {
+      R.sumv2 = 2.0 * R.ekin;
+      R.psi = (R.ethst == 'N') ? (R.sumv2 - R.nkt3_d) / R.Q : 0.0;
+      R.s = 0.0;
+      R.started = 1;
+      R.cstep = -1;
+    }
+    __syncthreads();
+  }
+  for (int w = 0; w < A.nwin; w++) {
+    if (R.done || R.status) break;
+    // wrt-csi.f:27 + chk_nucleation (main.f:157-161) at an analysis step
+    if (A.ftcsi > 0 && R.step % A.ftcsi == 0 && R.cstep != R.step) {
+      analysis<NT, SM>(R, C, A, P, R.step);
+      if (R.done) break;
+    }
+    const int nsteps = A.ftcsi > 0 ? A.ftcsi : 1;
+    for (int s = 0; s < nsteps; s++) {
+      if (R.step >= R.budget) {
+        if (tid == 0) R.done = 2;
+        __syncthreads();
+        break;
+      }
+      const bool last = (s == nsteps - 1);
+      const int step = R.step;
+      // drift
+      double d2 = 0.0, sv = 0.0;
+      const double psi = R.psi, dt2 = dt * dt / 2, dth = dt / 2;
+      for (int i = tid; i < N; i += NT) {
+        double vxi = A.vx[off + i], vyi = A.vy[off + i], vzi = A.vz[off + i];
+        double axi, ayi, azi;
+        get_a<MIXED>(A, off + i, axi, ayi, azi);
+        double dx, dy, dz;
+        if (!nh) {
+          double hx = 0.5 * axi * dt, hy = 0.5 * ayi * dt, hz = 0.5 * azi * dt;
+          dx = (vxi + hx) * dt;
+          dy = (vyi + hy) * dt;
+          dz = (vzi + hz) * dt;
+          vxi += hx;
+          vyi += hy;
+          vzi += hz;
+        } else {
+          dx = dt * vxi + dt2 * (axi - psi * vxi);
+          dy = dt * vyi + dt2 * (ayi - psi * vyi);
+          dz = dt * vzi + dt2 * (azi - psi * vzi);
+          sv += vxi * vxi + vyi * vyi + vzi * vzi;
+          vxi = vxi + dth * (axi - psi * vxi);
+          vyi = vyi + dth * (ayi - psi * vyi);
+          vzi = vzi + dth * (azi - psi * vzi);
+        }
+        P.set(i, P.x(i) + dx, P.y(i) + dy, P.z(i) + dz);
+        A.vx[off + i] = vxi;
+        A.vy[off + i] = vyi;
+        A.vz[off + i] = vzi;
+        d2 = fmax(d2, dx * dx + dy * dy + dz * dz);
+      }
+      double dmmr = cta_max<NT>(d2, C.red);
+      double sumv2 = nh ? cta_sum<NT>(sv, C.red) : 0.0;
+      if (tid == 0) {
+        if (nh) {
+          R.sumv2 = sumv2;
+          if (R.ethst == 'N') {
+            R.s = R.s + R.psi * dt + (R.sumv2 - R.nkt3_d) * dt2 / R.Q;
+            R.psi = R.psi + (R.sumv2 - R.nkt3_d) * dth / R.Q;
+          }
+        }
+        C.flag = 1;
+        if (skin(R, A, dmmr)) C.flag = prologue(R, C, A, step) ? 2 : 0;
+      }
+      __syncthreads();
+      if (C.flag == 0) goto out;
+      if (C.flag == 2 && !rebuild<NT, SM>(R, C, A, P)) goto out;
+      forces<NT, SM, MIXED>(R, C, A, P, !nh, last);
+      if (nh) {
+        // int-verlet-nh-mav.f:91-180 with block reductions
+        const double Q = R.Q, err = 1.0e-10;
+        const double psi1 = R.psi;
+        double s0 = 0.0;
+        for (int i = tid; i < N; i += NT) {
+          double a = A.vx[off + i], b = A.vy[off + i], c = A.vz[off + i];
+          A.vxn[off + i] = a;
+          A.vyn[off + i] = b;
+          A.vzn[off + i] = c;
+          s0 += a * a + b * b + c * c;
+        }
+        double sumv2n = cta_sum<NT>(s0, C.red);
+        double psn = psi1;
+        int ready = 0;
+        for (int iter = 1; iter <= 1000; iter++) {
+          double pso = psn, dp = 0.0;
+          for (int i = tid; i < N; i += NT) {
+            double ax, ay, az;
+            get_a<MIXED>(A, off + i, ax, ay, az);
+            double vo = A.vxn[off + i];
+            dp += (-dth * (ax - pso * vo) - (A.vx[off + i] - vo)) * vo * dt / Q;
+            vo = A.vyn[off + i];
+            dp += (-dth * (ay - pso * vo) - (A.vy[off + i] - vo)) * vo * dt / Q;
+            vo = A.vzn[off + i];
+            dp += (-dth * (az - pso * vo) - (A.vz[off + i] - vo)) * vo * dt / Q;
+          }
+          double delps = cta_sum<NT>(dp, C.red);
+          double di = -(pso * dth + 1);
+          delps = delps - di * ((-sumv2n + R.nkt3_i) * dth / Q - (psi1 - pso));
+          delps = delps / (-dt2 * sumv2n / Q + di);
+          double s2 = 0.0;
+          int nr = 0;
+          for (int i = tid; i < N; i += NT) {
+            double ax, ay, az;
+            get_a<MIXED>(A, off + i, ax, ay, az);
+            double V[3] = {A.vx[off + i], A.vy[off + i], A.vz[off + i]};
+            double a3[3] = {ax, ay, az};
+            double* vn[3] = {A.vxn, A.vyn, A.vzn};
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+              double vo = vn[d][off + i];
+              double b = -dth * (a3[d] - pso * vo) - (V[d] - vo);
+              double nx = vo + (b + dth * vo * delps) / di;
+              if (fabs((nx - vo) / nx) > err) nr = 1;
+              vn[d][off + i] = nx;
+              s2 += nx * nx;
+            }
+          }
+          sumv2n = cta_sum<NT>(s2, C.red);
+          nr = __syncthreads_or(nr);
+          psn = pso + delps;
+          if (!nr) {
+            ready = 1;
+            break;
+          }
+        }
+        if (!ready) {
+          if (tid == 0 && R.status == 0) R.status = CLMD_ERR_NH_NOCONVERGE;
+          __syncthreads();
+          goto out;
+        }
+        for (int i = tid; i < N; i += NT) {
+          A.vx[off + i] = A.vxn[off + i];
+          A.vy[off + i] = A.vyn[off + i];
+          A.vz[off + i] = A.vzn[off + i];
+        }
+        if (tid == 0) {
+          R.sumv2 = sumv2n;
+          R.psi = psn;
+          R.ekin = 0.5 * sumv2n;
+        }
+      }
+      if (tid == 0) R.step = step + 1;
+      __syncthreads();
+    }
+  }
+out:
+  __syncthreads();
+  if (SM) {
+    for (int i = tid; i < N; i += NT) {
+      A.x[off + i] = C.sx[i];
+      A.y[off + i] = C.sy[i];
+      A.z[off + i] = C.sz[i];
+    }
+  }
+  __syncthreads();
+}
+
+template <int NT, bool SM, bool MIXED>
+__global__ void __launch_bounds__(NT) k_ens(Args A) {
+  extern __shared__ double dsm[];
+  __shared__ Rep R;
+  __shared__ Cta C;
+  __shared__ int item;
+  for (;;) {
+    if (threadIdx.x == 0) item = atomicAdd(A.ctr, 1);
+    __syncthreads();
+    const int it = item;
+    if (it >= A.nitems) break;
+    const int r = A.items[it];
+    // replica record -> shared memory
+    {
+      const int* src = (const int*)(A.reps + r);
+      int* dst = (int*)&R;
+      for (int k = threadIdx.x; k < (int)(sizeof(Rep) / 4); k += NT) dst[k] = src[k];
+    }
+    if (threadIdx.x == 0) {
+      int nmax = R.natom;
+      const int ncell = A.ncmax * A.ncmax * A.ncmax;
+      C.rep = r;
+      C.cstart = (int*)dsm;
+      C.cfill = C.cstart + (ncell + 1);
+      double* p = (double*)(C.cfill + ncell + 1);
+      C.sx = SM ? p : nullptr;
+      C.sy = SM ? p + nmax : nullptr;
+      C.sz = SM ? p + 2 * nmax : nullptr;
+    }
+    __syncthreads();
+    if (!R.done && !R.status) run_window<NT, SM, MIXED>(R, C, A);
+    {
+      const int* src = (const int*)&R;
+      int* dst = (int*)(A.reps + r);
+      for (int k = threadIdx.x; k < (int)(sizeof(Rep) / 4); k += NT) dst[k] = src[k];
+    }
+    if (threadIdx.x == 0) A.summary[r] = make_int4(R.done, R.status, R.step, R.maxcs);
+    __syncthreads();
+  }
+}
+
+}  // namespace clmd_ens
+
+// ===========================================================================
+// host side
+// ===========================================================================
+using namespace clmd_ens;
+
+struct Range {
+  long long off, len;
+};
+
+struct clmd_ensemble {
+  clmd_ens_config cfg;
+  int dev = 0, nsm = 148;
+  cudaStream_t stream = nullptr;
+  Args A;
+  Rep* h_reps = nullptr;  // pinned mirror
+  std::vector<int> used;  // slot in use
+  std::vector<long long> slot_off;
+  std::vector<Range> free_list;
+  int* d_items = nullptr;
+  int* d_ctr = nullptr;
+  int* h_items = nullptr;  // pinned
+  int4* h_summary = nullptr;  // pinned copy of A.summary
+  bool reps_stale = false;    // h_reps older than the device records
+  long long launches = 0;
+  size_t smem_cap = 0;
+  int threads = 256;
+  std::mutex mu;
+};
+
+static int ck(cudaError_t e, const char* w) {
+  if (e == cudaSuccess) return CLMD_OK;
+  fprintf(stderr, "clmd_ens: %s: %s\n", w, cudaGetErrorString(e));
+  return e == cudaErrorMemoryAllocation ? CLMD_ERR_NOMEM : CLMD_ERR_CUDA;
+}
+#define ECK(call)                        \
+  do {                                   \
+    int _r = ck((call), #call);          \
+    if (_r) return _r;                   \
+  } while (0)
+
+static size_t smem_bytes(int nmax, int ncmax, bool sm) {
+  size_t nc = (size_t)ncmax * ncmax * ncmax;
+  return sizeof(int) * (2 * nc + 2) + (sm ? 3 * sizeof(double) * (size_t)nmax : 0);
+}
+
+// the largest cell grid that fits beside the resident positions (at least
+// 6^3 cells; positions go to global memory when even that does not fit)
+static int cells_for(size_t cap, int nmax, bool* sm) {
+  const size_t reserve = 8192;  // static shared memory of the kernel
+  for (int nc = kNcMax; nc >= 6; nc--)
+    if (smem_bytes(nmax, nc, true) + reserve <= cap) {
+      *sm = true;
+      return nc;
+    }
+  *sm = false;
+  return kNcMax;
+}
+
+extern "C" int clmd_ens_create(const clmd_ens_config* cfg, clmd_ensemble** out) {
+  if (!cfg || !out || cfg->max_atoms < 2 || cfg->max_replicas < 1 || cfg->dt <= 0 ||
+      cfg->rc <= 0 || cfg->rskin < cfg->rc || cfg->nbtim < 1)
+    return CLMD_ERR_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+    cudaGetLastError();
+    return CLMD_ERR_NO_DEVICE;
+  }
+  clmd_ensemble* E = new clmd_ensemble();
+  E->cfg = *cfg;
+  if (E->cfg.list_stride <= 0) E->cfg.list_stride = 96;
+  if (E->cfg.threads <= 0) E->cfg.threads = 256;
+  E->threads = E->cfg.threads;
+  ECK(cudaGetDevice(&E->dev));
+  ECK(cudaDeviceGetAttribute(&E->nsm, cudaDevAttrMultiProcessorCount, E->dev));
+  int optin = 0;
+  ECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, E->dev));
+  E->smem_cap = (size_t)optin;
+  ECK(cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking));
+  const long long P = cfg->max_atoms;
+  Args& A = E->A;
+  memset(&A, 0, sizeof(A));
+  A.pool = P;
+  ECK(cudaMalloc(&A.x, 8 * P)); ECK(cudaMalloc(&A.y, 8 * P)); ECK(cudaMalloc(&A.z, 8 * P));
+  ECK(cudaMalloc(&A.vx, 8 * P)); ECK(cudaMalloc(&A.vy, 8 * P)); ECK(cudaMalloc(&A.vz, 8 * P));
+  ECK(cudaMalloc(&A.vxn, 8 * P)); ECK(cudaMalloc(&A.vyn, 8 * P)); ECK(cudaMalloc(&A.vzn, 8 * P));
+  ECK(cudaMalloc(&A.a, 3 * 8 * P));
+  ECK(cudaMalloc(&A.list, 4 * P * (long long)E->cfg.list_stride));
+  ECK(cudaMalloc(&A.rlen, 4 * P)); ECK(cudaMalloc(&A.sorted, 4 * P));
+  ECK(cudaMalloc(&A.cellid, 4 * P)); ECK(cudaMalloc(&A.parent, 4 * P));
+  ECK(cudaMalloc(&A.cs, 4 * P)); ECK(cudaMalloc(&A.cl, 4 * P));
+  ECK(cudaMemset(A.a, 0, 3 * 8 * P));
+  ECK(cudaMemset(A.rlen, 0, 4 * P));
+  ECK(cudaMemset(A.cl, 0, 4 * P));
+  const int R = cfg->max_replicas;
+  ECK(cudaMalloc(&A.reps, sizeof(Rep) * R));
+  ECK(cudaMemset(A.reps, 0, sizeof(Rep) * R));
+  ECK(cudaMalloc(&A.fpt, sizeof(int) * kFptCap * R));
+  ECK(cudaMalloc(&A.summary, sizeof(int4) * R));
+  ECK(cudaMemset(A.summary, 0, sizeof(int4) * R));
+  ECK(cudaMallocHost(&E->h_summary, sizeof(int4) * R));
+  memset(E->h_summary, 0, sizeof(int4) * R);
+  ECK(cudaMallocHost(&E->h_reps, sizeof(Rep) * R));
+  memset(E->h_reps, 0, sizeof(Rep) * R);
+  ECK(cudaMalloc(&E->d_items, sizeof(int) * R));
+  ECK(cudaMalloc(&E->d_ctr, sizeof(int) * 4));
+  ECK(cudaMallocHost(&E->h_items, sizeof(int) * R));
+  A.items = E->d_items;
+  A.ctr = E->d_ctr;
+  A.rc = cfg->rc;
+  A.atskin = cfg->atskin;
+  A.dt = cfg->dt;
+  A.nbtim = cfg->nbtim;
+  A.ftcsi = cfg->ftcsi;
+  A.lstride = E->cfg.list_stride;
+  A.integrator = cfg->integrator;
+  E->used.assign(R, 0);
+  E->slot_off.assign(R, -1);
+  E->free_list.push_back({0, P});
+  *out = E;
+  return CLMD_OK;
+}
+
+extern "C" int clmd_ens_destroy(clmd_ensemble* E) {
+  if (!E) return CLMD_OK;
+  cudaStreamSynchronize(E->stream);
+  Args& A = E->A;
+  void* ps[] = {A.x, A.y, A.z, A.vx, A.vy, A.vz, A.vxn, A.vyn, A.vzn, A.a, A.list, A.rlen,
+                A.sorted, A.cellid, A.parent, A.cs, A.cl, A.reps, A.fpt, A.summary,
+                E->d_items, E->d_ctr};
+  for (void* p : ps)
+    if (p) cudaFree(p);
+  if (E->h_reps) cudaFreeHost(E->h_reps);
+  if (E->h_items) cudaFreeHost(E->h_items);
+  if (E->h_summary) cudaFreeHost(E->h_summary);
+  if (E->stream) cudaStreamDestroy(E->stream);
+  delete E;
+  return CLMD_OK;
+}
+
+static long long pool_alloc(clmd_ensemble* E, long long n) {
+  for (size_t k = 0; k < E->free_list.size(); k++) {
+    Range& r = E->free_list[k];
+    if (r.len >= n) {
+      long long off = r.off;
+      r.off += n;
+      r.len -= n;
+      if (r.len == 0) E->free_list.erase(E->free_list.begin() + k);
+      return off;
+    }
+  }
+  return -1;
+}
+
+static void pool_free(clmd_ensemble* E, long long off, long long n) {
+  E->free_list.push_back({off, n});
+  std::sort(E->free_list.begin(), E->free_list.end(),
+            [](const Range& a, const Range& b) { return a.off < b.off; });
+  std::vector<Range> m;
+  for (auto& r : E->free_list) {
+    if (!m.empty() && m.back().off + m.back().len == r.off)
+      m.back().len += r.len;
+    else
+      m.push_back(r);
+  }
+  E->free_list.swap(m);
+}
+
+static int refresh_reps(clmd_ensemble* E) {
+  if (!E->reps_stale) return CLMD_OK;
+  ECK(cudaMemcpyAsync(E->h_reps, E->A.reps, sizeof(Rep) * E->cfg.max_replicas,
+                      cudaMemcpyDeviceToHost, E->stream));
+  ECK(cudaStreamSynchronize(E->stream));
+  E->reps_stale = false;
+  return CLMD_OK;
+}
+
+extern "C" int64_t clmd_ens_free_atoms(clmd_ensemble* E) {
+  if (!E) return 0;
+  long long s = 0;
+  for (auto& r : E->free_list) s += r.len;
+  return s;
+}
+
+extern "C" int64_t clmd_ens_launches(clmd_ensemble* E) { return E ? E->launches : 0; }
+
+extern "C" int clmd_ens_add(clmd_ensemble* E, const clmd_replica_spec* sp, const double* x,
+                            const double* y, const double* z, const double* vx,
+                            const double* vy, const double* vz, int32_t* slot) {
+  if (!E || !sp || !x || !y || !z || !vx || !vy || !vz || !slot) return CLMD_ERR_ARG;
+  const int N = sp->natom;
+  if (N < 2 || !(sp->box > 2 * E->cfg.rc) || !(sp->temp > 0)) return CLMD_ERR_ARG;
+  std::lock_guard<std::mutex> lock(E->mu);
+  int s = -1;
+  for (int k = 0; k < E->cfg.max_replicas; k++)
+    if (!E->used[k]) {
+      s = k;
+      break;
+    }
+  if (s < 0) return CLMD_ERR_NOMEM;
+  long long off = pool_alloc(E, N);
+  if (off < 0) return CLMD_ERR_NOMEM;
+  Args& A = E->A;
+  cudaStream_t st = E->stream;
+  ECK(cudaMemcpyAsync(A.x + off, x, 8 * N, cudaMemcpyHostToDevice, st));
+  ECK(cudaMemcpyAsync(A.y + off, y, 8 * N, cudaMemcpyHostToDevice, st));
+  ECK(cudaMemcpyAsync(A.z + off, z, 8 * N, cudaMemcpyHostToDevice, st));
+  ECK(cudaMemcpyAsync(A.vx + off, vx, 8 * N, cudaMemcpyHostToDevice, st));
+  ECK(cudaMemcpyAsync(A.vy + off, vy, 8 * N, cudaMemcpyHostToDevice, st));
+  ECK(cudaMemcpyAsync(A.vz + off, vz, 8 * N, cudaMemcpyHostToDevice, st));
+  Rep& R = E->h_reps[s];
+  memset(&R, 0, sizeof(Rep));
+  R.box = sp->box;
+  R.ibox = 1.0 / sp->box;
+  R.att = sp->temp / CLMD_CIKB;
+  R.Q = sp->Q > 0 ? sp->Q : N * sp->temp * 0.25;
+  R.nkt3_i = (double)(3 * N) * CLMD_CIKB * R.att;
+  R.nkt3_d = 3.0 * N * CLMD_CIKB * R.att;
+  R.ekinT = 1.5 * CLMD_CIKB * R.att * N;
+  R.natom = N;
+  R.off = (int)off;
+  R.csover = sp->csover > 0 ? sp->csover : N + 1;
+  R.clwait = sp->clwait;
+  R.budget = sp->budget > 0 ? sp->budget : 0x7fffffff;
+  R.ethst = sp->ethst;
+  // read-3d.f:263-276
+  R.atrskin = E->cfg.rskin;
+  for (int i = 0; i < 256; i++)
+    R.dmmh[i] = (E->cfg.rskin - E->cfg.rc) / (double)(float)E->cfg.nbtim;
+  R.dmmsu = 256.0 * (E->cfg.rskin - E->cfg.rc) / (double)(float)E->cfg.nbtim;
+  R.cstep = -1;
+  ECK(cudaMemcpyAsync(A.reps + s, &R, sizeof(Rep), cudaMemcpyHostToDevice, st));
+  E->h_summary[s] = make_int4(0, 0, 0, 0);
+  ECK(cudaMemcpyAsync(A.summary + s, &E->h_summary[s], sizeof(int4), cudaMemcpyHostToDevice,
+                      st));
+  std::vector<int> neg(kFptCap, -1);
+  ECK(cudaMemcpyAsync(A.fpt + (size_t)s * kFptCap, neg.data(), sizeof(int) * kFptCap,
+                      cudaMemcpyHostToDevice, st));
+  ECK(cudaStreamSynchronize(st));
+  E->used[s] = 1;
+  E->slot_off[s] = off;
+  *slot = s;
+  return CLMD_OK;
+}
+
+extern "C" int clmd_ens_remove(clmd_ensemble* E, int32_t slot) {
+  if (!E || slot < 0 || slot >= E->cfg.max_replicas || !E->used[slot]) return CLMD_ERR_ARG;
+  std::lock_guard<std::mutex> lock(E->mu);
+  ECK(cudaStreamSynchronize(E->stream));
+  int rs = refresh_reps(E);
+  if (rs) return rs;
+  pool_free(E, E->slot_off[slot], E->h_reps[slot].natom);
+  E->used[slot] = 0;
+  E->slot_off[slot] = -1;
+  memset(&E->h_reps[slot], 0, sizeof(Rep));
+  E->h_reps[slot].done = 3;  // free
+  E->h_summary[slot] = make_int4(3, 0, 0, 0);
+  ECK(cudaMemcpyAsync(E->A.reps + slot, &E->h_reps[slot], sizeof(Rep), cudaMemcpyHostToDevice,
+                      E->stream));
+  ECK(cudaStreamSynchronize(E->stream));
+  return CLMD_OK;
+}
+
+typedef void (*EnsKernel)(Args);
+
+template <int NT>
+static EnsKernel pick(bool sm, bool mixed) {
+  if (sm) return mixed ? k_ens<NT, true, true> : k_ens<NT, true, false>;
+  return mixed ? k_ens<NT, false, true> : k_ens<NT, false, false>;
+}
+
+static EnsKernel kernel_for(int nt, bool sm, bool mixed) {
+  switch (nt) {
+    case 128: return pick<128>(sm, mixed);
+    case 512: return pick<512>(sm, mixed);
+    case 1024: return pick<1024>(sm, mixed);
+    default: return pick<256>(sm, mixed);
+  }
+}
+
+// one launch: every listed replica advances by nwin windows
+static int launch(clmd_ensemble* E, const std::vector<int>& items, int nmax, int nwin) {
+  if (items.empty()) return CLMD_OK;
+  const bool mixed = E->cfg.precision == CLMD_PREC_MIXED;
+  bool sm = false;
+  const int ncmax = cells_for(E->smem_cap, nmax, &sm);
+  size_t smem = smem_bytes(nmax, ncmax, sm);
+  const int nt = E->threads;
+  EnsKernel k = kernel_for(nt, sm, mixed);
+  ECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  ECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, nt, smem));
+  if (per_sm < 1) return CLMD_ERR_ARG;
+  int grid = std::min<long long>((long long)per_sm * E->nsm, (long long)items.size());
+  memcpy(E->h_items, items.data(), sizeof(int) * items.size());
+  ECK(cudaMemcpyAsync(E->d_items, E->h_items, sizeof(int) * items.size(),
+                      cudaMemcpyHostToDevice, E->stream));
+  ECK(cudaMemsetAsync(E->d_ctr, 0, sizeof(int), E->stream));
+  Args A = E->A;
+  A.nitems = (int)items.size();
+  A.nwin = nwin;
+  A.ncmax = ncmax;
+  k<<<grid, nt, smem, E->stream>>>(A);
+  E->launches++;
+  return ck(cudaGetLastError(), "k_ens launch");
+}
+
+extern "C" int clmd_ens_step(clmd_ensemble* E, int32_t nwin) {
+  if (!E || nwin < 1) return CLMD_ERR_ARG;
+  std::lock_guard<std::mutex> lock(E->mu);
+  // running replicas, largest first (longest-processing-time order)
+  std::vector<int> items;
+  int nmax = 0;
+  for (int s = 0; s < E->cfg.max_replicas; s++)
+    if (E->used[s] && !E->h_summary[s].x && !E->h_summary[s].y) {
+      items.push_back(s);
+      nmax = std::max(nmax, E->h_reps[s].natom);
+    }
+  std::sort(items.begin(), items.end(), [&](int a, int b) {
+    return E->h_reps[a].natom != E->h_reps[b].natom ? E->h_reps[a].natom > E->h_reps[b].natom
+                                                    : a < b;
+  });
+  int st = launch(E, items, nmax, nwin);
+  if (st) return st;
+  ECK(cudaMemcpyAsync(E->h_summary, E->A.summary, sizeof(int4) * E->cfg.max_replicas,
+                      cudaMemcpyDeviceToHost, E->stream));
+  ECK(cudaStreamSynchronize(E->stream));
+  E->reps_stale = true;
+  return CLMD_OK;
+}
+
+extern "C" int clmd_ens_results(clmd_ensemble* E, clmd_replica_result* out, int32_t cap,
+                                int32_t* n) {
+  if (!E || !n) return CLMD_ERR_ARG;
+  std::lock_guard<std::mutex> lock(E->mu);
+  int rs = refresh_reps(E);
+  if (rs) return rs;
+  int k = 0;
+  for (int s = 0; s < E->cfg.max_replicas; s++) {
+    if (!E->used[s]) continue;
+    if (out && k < cap) {
+      const Rep& R = E->h_reps[s];
+      clmd_replica_result& o = out[k];
+      o.ekin = R.ekin;
+      o.epot = R.epot;
+      o.psi = R.psi;
+      o.s = R.s;
+      o.slot = s;
+      o.natom = R.natom;
+      o.step = R.step;
+      o.status = R.status;
+      o.done = R.done;
+      o.clbrkt = R.clbrkt;
+      o.maxcs = R.maxcs;
+      o.nrebuild = R.nrebuild;
+    }
+    k++;
+  }
+  *n = k;
+  return CLMD_OK;
+}
+
+extern "C" int clmd_ens_get_state(clmd_ensemble* E, int32_t slot, double* x, double* y,
+                                  double* z, double* vx, double* vy, double* vz, double* ax,
+                                  double* ay, double* az, int32_t* cl) {
+  if (!E || slot < 0 || slot >= E->cfg.max_replicas || !E->used[slot]) return CLMD_ERR_ARG;
+  std::lock_guard<std::mutex> lock(E->mu);
+  const Args& A = E->A;
+  const long long off = E->slot_off[slot];
+  const int N = E->h_reps[slot].natom;
+  cudaStream_t st = E->stream;
+  double* dst[6] = {x, y, z, vx, vy, vz};
+  double* src[6] = {A.x, A.y, A.z, A.vx, A.vy, A.vz};
+  for (int k = 0; k < 6; k++)
+    if (dst[k]) ECK(cudaMemcpyAsync(dst[k], src[k] + off, 8 * N, cudaMemcpyDeviceToHost, st));
+  double* ad[3] = {ax, ay, az};
+  if (E->cfg.precision == CLMD_PREC_MIXED) {
+    std::vector<float> tmp(N);
+    for (int k = 0; k < 3; k++)
+      if (ad[k]) {
+        ECK(cudaMemcpyAsync(tmp.data(), (float*)A.a + k * A.pool + off, 4 * N,
+                            cudaMemcpyDeviceToHost, st));
+        ECK(cudaStreamSynchronize(st));
+        for (int i = 0; i < N; i++) ad[k][i] = tmp[i];
+      }
+  } else {
+    for (int k = 0; k < 3; k++)
+      if (ad[k])
+        ECK(cudaMemcpyAsync(ad[k], (double*)A.a + k * A.pool + off, 8 * N,
+                            cudaMemcpyDeviceToHost, st));
+  }
+  if (cl) ECK(cudaMemcpyAsync(cl, A.cl + off, 4 * N, cudaMemcpyDeviceToHost, st));
+  ECK(cudaStreamSynchronize(st));
+  return CLMD_OK;
+}
+
+extern "C" int clmd_ens_fpt(clmd_ensemble* E, int32_t slot, int32_t* fpt, int32_t cap) {
+  if (!E || !fpt || slot < 0 || slot >= E->cfg.max_replicas || !E->used[slot])
+    return CLMD_ERR_ARG;
+  int n = std::min(cap, kFptCap);
+  ECK(cudaMemcpy(fpt, E->A.fpt + (size_t)slot * kFptCap, sizeof(int) * n,
+                 cudaMemcpyDeviceToHost));
+  for (int k = n; k < cap; k++) fpt[k] = -1;
+  return CLMD_OK;
+}

@@ -212,6 +212,81 @@ int clmd_init_random(int32_t n, double boxx, double boxy, double boxz, double rm
                      double kT_over_m, uint64_t seed, double* x, double* y, double* z,
                      double* vx, double* vy, double* vz);
 
+/* ---------------------------------------------------------------------------
+ * Ensembles: many independent replicas (configs "batched" and "served") in
+ * one persistent launch.  Reduced LJ units (sigma = eps = m = 1, one
+ * species), the same per-replica algorithm as the drop-in (adaptive-skin
+ * Verlet list, velocity Verlet or Nose-Hoover, Stillinger analysis every
+ * ftcsi steps, chk_nucleation), with FP32 pair terms accumulated per atom in
+ * FP32 with Kahan compensation (CLMD_PREC_MIXED) or all FP64.  Replicas are
+ * admitted while the atom pool has room and run window by window (one
+ * analysis + ftcsi steps), finished ones are retired: continuous batching.
+ * ------------------------------------------------------------------------- */
+typedef struct clmd_ens_config {
+  double rc, rskin, atskin, dt;  /* sigma units: cut-off, initial list radius, cluster radius */
+  int64_t max_atoms;             /* atom pool (the admission budget) */
+  int32_t max_replicas;
+  int32_t list_stride;           /* neighbour slots per atom; 0 = autotune */
+  int32_t precision;             /* CLMD_PREC_MIXED or CLMD_PREC_FP64 */
+  int32_t integrator;            /* CLMD_INT_VERLET or CLMD_INT_NOSE */
+  int32_t ftcsi;                 /* steps per window (between cluster analyses) */
+  int32_t nbtim;                 /* target steps between list rebuilds */
+  int32_t threads;               /* threads per replica (CTA size); 0 = autotune */
+  int32_t pad;
+} clmd_ens_config;
+
+typedef struct clmd_replica_spec {
+  double box;        /* cubic box edge */
+  double temp;       /* T* */
+  double Q;          /* Nose-Hoover mass (reduced), <= 0: N T* 0.25 */
+  int32_t natom;
+  int32_t csover;    /* nucleated once a cluster >= csover persists (chk-nucleation.f) */
+  int32_t clwait;
+  int32_t budget;    /* step budget */
+  char ethst;        /* 'N' Nose-Hoover thermostat on, '-' off */
+  char pad[7];
+} clmd_replica_spec;
+
+typedef struct clmd_replica_result {
+  double ekin, epot, psi, s;
+  int32_t slot, natom, step, status;
+  int32_t done;        /* 1 nucleated, 2 budget spent, 0 running */
+  int32_t clbrkt;      /* first step the >= csover cluster was seen (time to nucleation) */
+  int32_t maxcs;       /* largest cluster at the last analysis */
+  int32_t nrebuild;
+} clmd_replica_result;
+
+typedef struct clmd_ensemble clmd_ensemble;
+
+int clmd_ens_create(const clmd_ens_config* cfg, clmd_ensemble** out);
+int clmd_ens_destroy(clmd_ensemble* e);
+/* Admits a replica from host positions/velocities (x..vz, natom each): the
+ * reference's start (stopdead(-1), neighbor(0), AccAtom, and main.f:156-160
+ * for PSI) runs on the device at the next step call.  *slot gets its id.
+ * CLMD_ERR_NOMEM when the pool or the replica table has no room now. */
+int clmd_ens_add(clmd_ensemble* e, const clmd_replica_spec* spec, const double* x,
+                 const double* y, const double* z, const double* vx, const double* vy,
+                 const double* vz, int32_t* slot);
+/* Advances every running replica by up to nwin windows (one launch per
+ * window, replayed from a CUDA graph); replicas stop when done. */
+int clmd_ens_step(clmd_ensemble* e, int32_t nwin);
+/* Per-slot results of all occupied slots (n gets the count). */
+int clmd_ens_results(clmd_ensemble* e, clmd_replica_result* out, int32_t cap, int32_t* n);
+/* Frees a finished (or unwanted) replica's pool range and slot. */
+int clmd_ens_remove(clmd_ensemble* e, int32_t slot);
+/* Copies one replica's state (x..vz, ax..az, cluster labels cl, 1-based) out;
+ * any pointer may be NULL. */
+int clmd_ens_get_state(clmd_ensemble* e, int32_t slot, double* x, double* y, double* z,
+                       double* vx, double* vy, double* vz, double* ax, double* ay,
+                       double* az, int32_t* cl);
+/* First step at which the largest cluster reached each size 1..cap (-1 if
+ * not yet). */
+int clmd_ens_fpt(clmd_ensemble* e, int32_t slot, int32_t* fpt, int32_t cap);
+/* Atoms currently free in the pool. */
+int64_t clmd_ens_free_atoms(clmd_ensemble* e);
+/* Kernel launches issued so far. */
+int64_t clmd_ens_launches(clmd_ensemble* e);
+
 /* No counterpart in the reference: the Stillinger analysis (what stoddard()
  * of stoddard-pbc-n-m.f computes: labels cl, sizes cs, histogram csi) for
  * callers that cannot let the library allocate device memory -- hosts that
