@@ -408,6 +408,105 @@ def engine_arm(args, w):
         torch.distributed.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# batched ensemble (configs "batched"): mixed precision vs the FP64 drop-in
+# ---------------------------------------------------------------------------
+def ensemble_specs(nrep, seed, nmin=200, nmax=8000):
+    rng = np.random.default_rng(seed)
+    n = np.exp(rng.uniform(np.log(nmin), np.log(nmax), nrep)).astype(int)
+    rho = rng.uniform(0.01, 0.05, nrep)
+    temp = rng.uniform(0.65, 0.85, nrep)
+    return [(int(n[k]), float(rho[k]), float(temp[k]), seed * 100003 + k) for k in range(nrep)]
+
+
+def dropin_rate(n, rho, temp, seed, steps=300):
+    """atom-steps/s of the FP64 drop-in (one system per launch sequence) on
+    one replica: Nose-Hoover, Stillinger every 100 steps."""
+    import torch
+    cfg = clmd.lj_config(n, rho, temp, integrator=clmd.INT_NOSE, ethst="N", ftcsi=100)
+    st = make_state(cfg, seed, temp)
+    g = start_system(cfg, st)
+    s = g.scalars()
+    sumv2 = 2.0 * s.ekin
+    s.psi = (sumv2 - 3.0 * n * clmd.CIKB * cfg.att) / cfg.Q
+    g.set_scalars(s)
+    g.run(0, 100)
+    stream = torch.cuda.ExternalStream(g.stream())
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    g.run(100, steps)
+    b.record(stream)
+    b.synchronize()
+    ms = a.elapsed_time(b)
+    g.close()
+    return n * steps / (ms / 1e3)
+
+
+def batched_arm(args):
+    import torch
+    torch.cuda.set_device(0)
+    clmd.set_device(0)
+    specs = ensemble_specs(args.replicas, 7)
+    total = sum(sp[0] for sp in specs)
+    e = clmd.Ensemble(clmd.ens_config(total + 1024, len(specs), precision=clmd.PREC_MIXED,
+                                      integrator=clmd.INT_NOSE, ftcsi=100,
+                                      threads=args.threads))
+    t0 = time.perf_counter()
+    slots = {}
+    for n, rho, temp, sd in specs:
+        box = (n / rho) ** (1.0 / 3.0)
+        x, y, z, vx, vy, vz = clmd.init_random(n, (box, box, box), 0.9, temp, sd)
+        slots[e.add(n, box, temp, x, y, z, vx, vy, vz, csover=51, clwait=0,
+                    budget=200000)] = (n, rho, temp, sd)
+    log(f"admitted {len(slots)} replicas, {total} atoms in {time.perf_counter()-t0:.1f} s")
+    e.step(1)  # start sequences + first window (warm-up)
+    for _ in range(args.warmup - 1):
+        e.step(1)
+    tuned = e.autotune() if args.threads == 0 else [args.threads] * 4
+    r0 = {k: v.step for k, v in e.results().items()}
+    torch.cuda.synchronize()
+    l0 = e.launches()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        e.step(1)
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t
+    res = e.results()
+    atom_steps = sum(slots[k][0] * (res[k].step - r0[k]) for k in slots)
+    value = atom_steps / el
+    done = sum(1 for r in res.values() if r.done == 1)
+    # the FP64 drop-in on the same ensemble: per-replica rates on a stratified
+    # sample, total time for every replica's steps, same atom-steps
+    order = sorted(slots, key=lambda k: slots[k][0])
+    picks = [order[int(q * (len(order) - 1))] for q in np.linspace(0, 1, args.dropin_sample)]
+    rates = []
+    for k in picks:
+        n, rho, temp, sd = slots[k]
+        rates.append((n, dropin_rate(n, rho, temp, sd)))
+    ln = np.log([r[0] for r in rates])
+    lr = np.log([r[1] for r in rates])
+    t_drop = 0.0
+    for k in slots:
+        n = slots[k][0]
+        rate = float(np.exp(np.interp(np.log(n), ln, lr)))
+        t_drop += n * (res[k].step - r0[k]) / rate
+    dropin_value = atom_steps / t_drop
+    line = {
+        "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic (seeded)",
+        "config": {"workload": f"batched-{len(slots)}-replicas-N200-8000-NH-mixed",
+                   "replicas": len(slots), "atoms": total, "steps_per_bench_step": 100,
+                   "threads_per_size_class": tuned, "parallelism": "replicas"},
+        "fp64_dropin_same_ensemble": dropin_value,
+        "speedup_vs_fp64_dropin": value / dropin_value,
+        "dropin_sample_rates": [[n, r] for n, r in rates],
+        "nucleated": done, "gpu_launches": int(e.launches() - l0),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -416,8 +515,15 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--natom", type=int, default=WORKLOAD["natom"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="dropin", choices=["dropin", "batched"])
+    ap.add_argument("--replicas", type=int, default=4096)
+    ap.add_argument("--threads", type=int, default=0, help="0 = autotune")
+    ap.add_argument("--dropin-sample", type=int, default=8)
     args = ap.parse_args()
     w = dict(WORKLOAD, natom=args.natom)
+    if args.workload == "batched":
+        batched_arm(args)
+        return
     if args.impl == "reference":
         reference_arm(args, w)
     else:

@@ -245,6 +245,7 @@ def load(path: str = LIB_PATH):
         "clmd_ens_destroy": ([P], C.c_int),
         "clmd_ens_add": ([P, C.POINTER(ReplicaSpec), d, d, d, d, d, d, i], C.c_int),
         "clmd_ens_step": ([P, C.c_int32], C.c_int),
+        "clmd_ens_autotune": ([P, i], C.c_int),
         "clmd_ens_results": ([P, C.POINTER(ReplicaResult), C.c_int32, i], C.c_int),
         "clmd_ens_remove": ([P, C.c_int32], C.c_int),
         "clmd_ens_get_state": ([P, C.c_int32, d, d, d, d, d, d, d, d, d, i], C.c_int),
@@ -550,6 +551,14 @@ class Ensemble:
         st = self.lib.clmd_ens_step(self.h, nwin)
         if st:
             raise ClmdError(st, "clmd_ens_step")
+
+    def autotune(self):
+        """Block size per replica-size class, picked by timing (4 windows)."""
+        out = (C.c_int32 * 4)()
+        st = self.lib.clmd_ens_autotune(self.h, out)
+        if st:
+            raise ClmdError(st, "clmd_ens_autotune")
+        return list(out)
 
     def results(self):
         cap = len(self.natom) + 1

@@ -46,7 +46,7 @@ struct Rep {
   double atrskin, dmms, dmmsu, dmmax, dmmav;
   double dmmh[256];
   int dmmst, dmmi, step, status, done, clbrkt, maxcs, fpt_top, nrebuild, cstep, started;
-  int pad;
+  int ncmax;  // cell-grid cap, fixed at admission from this replica's size only
 };
 
 struct Args {
@@ -157,7 +157,7 @@ struct Pos {
 
 // neighbor-pbc-mav.f:48-60, 101-105 on the replica record (thread 0)
 __device__ bool prologue(Rep& R, Cta& C, const Args& A, int step) {
-  const int kNcMax = A.ncmax;
+  const int kNcMax = R.ncmax;
   if (R.dmms > (R.atrskin - A.rc)) {
     if (R.status == 0) R.status = CLMD_ERR_SKIN;
     return false;
@@ -577,7 +577,7 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
   // the grid of the current list
   if (tid == 0) {
     int n = (int)floor(R.box / (R.atrskin * (1.0 + 1e-9)));
-    n = max(1, min(n, A.ncmax));
+    n = max(1, min(n, R.ncmax));
     C.ncx = n;
     C.ncell = n * n * n;
     C.cf = (double)n / R.box;
@@ -777,7 +777,7 @@ __global__ void __launch_bounds__(NT) k_ens(Args A) {
     }
     if (threadIdx.x == 0) {
       int nmax = R.natom;
-      const int ncell = A.ncmax * A.ncmax * A.ncmax;
+      const int ncell = R.ncmax * R.ncmax * R.ncmax;
       C.rep = r;
       C.cstart = (int*)dsm;
       C.cfill = C.cstart + (ncell + 1);
@@ -823,6 +823,15 @@ struct clmd_ensemble {
   int* h_items = nullptr;  // pinned
   int4* h_summary = nullptr;  // pinned copy of A.summary
   bool reps_stale = false;    // h_reps older than the device records
+  // size classes: each has its own block size, shared-memory budget, stream
+  static constexpr int kClasses = 4;
+  int cls_max[kClasses] = {1024, 2560, 6144, 1 << 30};
+  int cls_threads[kClasses] = {128, 256, 512, 1024};
+  cudaStream_t cstream[kClasses] = {};
+  cudaEvent_t ev0[kClasses] = {}, ev1[kClasses] = {}, evj = nullptr;
+  float last_ms[kClasses] = {};
+  long long last_atoms[kClasses] = {};
+  bool tuned = false;
   long long launches = 0;
   size_t smem_cap = 0;
   int threads = 256;
@@ -878,6 +887,14 @@ extern "C" int clmd_ens_create(const clmd_ens_config* cfg, clmd_ensemble** out) 
   ECK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, E->dev));
   E->smem_cap = (size_t)optin;
   ECK(cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking));
+  for (int c = 0; c < clmd_ensemble::kClasses; c++) {
+    ECK(cudaStreamCreateWithFlags(&E->cstream[c], cudaStreamNonBlocking));
+    ECK(cudaEventCreate(&E->ev0[c]));
+    ECK(cudaEventCreate(&E->ev1[c]));
+    if (cfg->threads > 0) E->cls_threads[c] = cfg->threads;
+  }
+  ECK(cudaEventCreateWithFlags(&E->evj, cudaEventDisableTiming));
+  E->tuned = cfg->threads > 0;
   const long long P = cfg->max_atoms;
   Args& A = E->A;
   memset(&A, 0, sizeof(A));
@@ -904,7 +921,7 @@ extern "C" int clmd_ens_create(const clmd_ens_config* cfg, clmd_ensemble** out) 
   ECK(cudaMallocHost(&E->h_reps, sizeof(Rep) * R));
   memset(E->h_reps, 0, sizeof(Rep) * R);
   ECK(cudaMalloc(&E->d_items, sizeof(int) * R));
-  ECK(cudaMalloc(&E->d_ctr, sizeof(int) * 4));
+  ECK(cudaMalloc(&E->d_ctr, sizeof(int) * 16));
   ECK(cudaMallocHost(&E->h_items, sizeof(int) * R));
   A.items = E->d_items;
   A.ctr = E->d_ctr;
@@ -935,6 +952,12 @@ extern "C" int clmd_ens_destroy(clmd_ensemble* E) {
   if (E->h_items) cudaFreeHost(E->h_items);
   if (E->h_summary) cudaFreeHost(E->h_summary);
   if (E->stream) cudaStreamDestroy(E->stream);
+  for (int c = 0; c < clmd_ensemble::kClasses; c++) {
+    if (E->cstream[c]) cudaStreamDestroy(E->cstream[c]);
+    if (E->ev0[c]) cudaEventDestroy(E->ev0[c]);
+    if (E->ev1[c]) cudaEventDestroy(E->ev1[c]);
+  }
+  if (E->evj) cudaEventDestroy(E->evj);
   delete E;
   return CLMD_OK;
 }
@@ -1030,6 +1053,8 @@ extern "C" int clmd_ens_add(clmd_ensemble* E, const clmd_replica_spec* sp, const
     R.dmmh[i] = (E->cfg.rskin - E->cfg.rc) / (double)(float)E->cfg.nbtim;
   R.dmmsu = 256.0 * (E->cfg.rskin - E->cfg.rc) / (double)(float)E->cfg.nbtim;
   R.cstep = -1;
+  bool fits = false;
+  R.ncmax = cells_for(E->smem_cap, N, &fits);
   ECK(cudaMemcpyAsync(A.reps + s, &R, sizeof(Rep), cudaMemcpyHostToDevice, st));
   E->h_summary[s] = make_int4(0, 0, 0, 0);
   ECK(cudaMemcpyAsync(A.summary + s, &E->h_summary[s], sizeof(int4), cudaMemcpyHostToDevice,
@@ -1079,55 +1104,142 @@ static EnsKernel kernel_for(int nt, bool sm, bool mixed) {
   }
 }
 
-// one launch: every listed replica advances by nwin windows
-static int launch(clmd_ensemble* E, const std::vector<int>& items, int nmax, int nwin) {
-  if (items.empty()) return CLMD_OK;
+// one launch of one size class: every listed replica advances by nwin
+// windows; items[] is the class's slice of the device item list
+static int launch_class(clmd_ensemble* E, int c, int item0, int nitems, const int* slots,
+                        int nwin, int nt) {
+  if (nitems == 0) return CLMD_OK;
   const bool mixed = E->cfg.precision == CLMD_PREC_MIXED;
-  bool sm = false;
-  const int ncmax = cells_for(E->smem_cap, nmax, &sm);
-  size_t smem = smem_bytes(nmax, ncmax, sm);
-  const int nt = E->threads;
+  // positions stay in shared memory if every replica of the class fits
+  bool sm = true;
+  for (int k = 0; k < nitems; k++) {
+    const Rep& R = E->h_reps[slots[k]];
+    if (smem_bytes(R.natom, R.ncmax, true) + 8192 > E->smem_cap) sm = false;
+  }
+  size_t smem = 0;
+  int ncmax = 1;
+  for (int k = 0; k < nitems; k++) {
+    const Rep& R = E->h_reps[slots[k]];
+    smem = std::max(smem, smem_bytes(R.natom, R.ncmax, sm));
+    ncmax = std::max(ncmax, R.ncmax);
+  }
   EnsKernel k = kernel_for(nt, sm, mixed);
   ECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   ECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, nt, smem));
   if (per_sm < 1) return CLMD_ERR_ARG;
-  int grid = std::min<long long>((long long)per_sm * E->nsm, (long long)items.size());
-  memcpy(E->h_items, items.data(), sizeof(int) * items.size());
-  ECK(cudaMemcpyAsync(E->d_items, E->h_items, sizeof(int) * items.size(),
-                      cudaMemcpyHostToDevice, E->stream));
-  ECK(cudaMemsetAsync(E->d_ctr, 0, sizeof(int), E->stream));
+  int grid = (int)std::min<long long>((long long)per_sm * E->nsm, (long long)nitems);
+  cudaStream_t st = E->cstream[c];
+  ECK(cudaMemsetAsync(E->d_ctr + c, 0, sizeof(int), st));
   Args A = E->A;
-  A.nitems = (int)items.size();
+  A.items = E->d_items + item0;
+  A.ctr = E->d_ctr + c;
+  A.nitems = nitems;
   A.nwin = nwin;
   A.ncmax = ncmax;
-  k<<<grid, nt, smem, E->stream>>>(A);
+  ECK(cudaEventRecord(E->ev0[c], st));
+  k<<<grid, nt, smem, st>>>(A);
+  ECK(cudaEventRecord(E->ev1[c], st));
   E->launches++;
   return ck(cudaGetLastError(), "k_ens launch");
+}
+
+// all running replicas, split by size class, each class largest first; the
+// classes run concurrently on their own streams
+static int launch_all(clmd_ensemble* E, int nwin, const int* threads) {
+  std::vector<int> cls[clmd_ensemble::kClasses];
+  int nmax[clmd_ensemble::kClasses] = {};
+  for (int s = 0; s < E->cfg.max_replicas; s++)
+    if (E->used[s] && !E->h_summary[s].x && !E->h_summary[s].y) {
+      int n = E->h_reps[s].natom, c = 0;
+      while (c < clmd_ensemble::kClasses - 1 && n > E->cls_max[c]) c++;
+      cls[c].push_back(s);
+      nmax[c] = std::max(nmax[c], n);
+    }
+  int total = 0;
+  for (int c = 0; c < clmd_ensemble::kClasses; c++) {
+    std::sort(cls[c].begin(), cls[c].end(), [&](int a, int b) {
+      return E->h_reps[a].natom != E->h_reps[b].natom
+                 ? E->h_reps[a].natom > E->h_reps[b].natom
+                 : a < b;
+    });
+    memcpy(E->h_items + total, cls[c].data(), sizeof(int) * cls[c].size());
+    total += (int)cls[c].size();
+  }
+  if (total == 0) return CLMD_OK;
+  ECK(cudaMemcpyAsync(E->d_items, E->h_items, sizeof(int) * total, cudaMemcpyHostToDevice,
+                      E->stream));
+  ECK(cudaEventRecord(E->evj, E->stream));
+  int off = 0;
+  for (int c = 0; c < clmd_ensemble::kClasses; c++) {
+    E->last_atoms[c] = 0;
+    for (int s : cls[c]) E->last_atoms[c] += E->h_reps[s].natom;
+    if (!cls[c].empty()) {
+      ECK(cudaStreamWaitEvent(E->cstream[c], E->evj, 0));
+      int st = launch_class(E, c, off, (int)cls[c].size(), cls[c].data(), nwin, threads[c]);
+      if (st) return st;
+    }
+    off += (int)cls[c].size();
+  }
+  for (int c = 0; c < clmd_ensemble::kClasses; c++) {
+    if (cls[c].empty()) {
+      E->last_ms[c] = -1.0f;
+      continue;
+    }
+    ECK(cudaStreamWaitEvent(E->stream, E->ev1[c], 0));
+  }
+  ECK(cudaMemcpyAsync(E->h_summary, E->A.summary, sizeof(int4) * E->cfg.max_replicas,
+                      cudaMemcpyDeviceToHost, E->stream));
+  ECK(cudaStreamSynchronize(E->stream));
+  for (int c = 0; c < clmd_ensemble::kClasses; c++)
+    if (!cls[c].empty()) ECK(cudaEventElapsedTime(&E->last_ms[c], E->ev0[c], E->ev1[c]));
+  E->reps_stale = true;
+  return CLMD_OK;
+}
+
+// Picks the block size of each size class from {128, 256, 512, 1024} by
+// timing one window per candidate on the running replicas (the trial
+// windows advance the simulation like any other window).
+static int autotune(clmd_ensemble* E) {
+  const int cand[4] = {128, 256, 512, 1024};
+  float best[clmd_ensemble::kClasses];
+  int pick[clmd_ensemble::kClasses];
+  for (int c = 0; c < clmd_ensemble::kClasses; c++) {
+    best[c] = 1e30f;
+    pick[c] = E->cls_threads[c];
+  }
+  for (int k = 0; k < 4; k++) {
+    int th[clmd_ensemble::kClasses];
+    for (int c = 0; c < clmd_ensemble::kClasses; c++) th[c] = cand[k];
+    int st = launch_all(E, 1, th);
+    if (st) return st;
+    for (int c = 0; c < clmd_ensemble::kClasses; c++) {
+      if (E->last_ms[c] < 0 || E->last_atoms[c] == 0) continue;
+      float per_atom = E->last_ms[c] / (float)E->last_atoms[c];
+      if (per_atom < best[c]) {
+        best[c] = per_atom;
+        pick[c] = cand[k];
+      }
+    }
+  }
+  for (int c = 0; c < clmd_ensemble::kClasses; c++) E->cls_threads[c] = pick[c];
+  E->tuned = true;
+  return CLMD_OK;
 }
 
 extern "C" int clmd_ens_step(clmd_ensemble* E, int32_t nwin) {
   if (!E || nwin < 1) return CLMD_ERR_ARG;
   std::lock_guard<std::mutex> lock(E->mu);
-  // running replicas, largest first (longest-processing-time order)
-  std::vector<int> items;
-  int nmax = 0;
-  for (int s = 0; s < E->cfg.max_replicas; s++)
-    if (E->used[s] && !E->h_summary[s].x && !E->h_summary[s].y) {
-      items.push_back(s);
-      nmax = std::max(nmax, E->h_reps[s].natom);
-    }
-  std::sort(items.begin(), items.end(), [&](int a, int b) {
-    return E->h_reps[a].natom != E->h_reps[b].natom ? E->h_reps[a].natom > E->h_reps[b].natom
-                                                    : a < b;
-  });
-  int st = launch(E, items, nmax, nwin);
-  if (st) return st;
-  ECK(cudaMemcpyAsync(E->h_summary, E->A.summary, sizeof(int4) * E->cfg.max_replicas,
-                      cudaMemcpyDeviceToHost, E->stream));
-  ECK(cudaStreamSynchronize(E->stream));
-  E->reps_stale = true;
-  return CLMD_OK;
+  return launch_all(E, nwin, E->cls_threads);
+}
+
+extern "C" int clmd_ens_autotune(clmd_ensemble* E, int32_t* threads_out) {
+  if (!E) return CLMD_ERR_ARG;
+  std::lock_guard<std::mutex> lock(E->mu);
+  int st = autotune(E);
+  if (threads_out)
+    for (int c = 0; c < clmd_ensemble::kClasses; c++) threads_out[c] = E->cls_threads[c];
+  return st;
 }
 
 extern "C" int clmd_ens_results(clmd_ensemble* E, clmd_replica_result* out, int32_t cap,

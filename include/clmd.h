@@ -270,6 +270,13 @@ int clmd_ens_add(clmd_ensemble* e, const clmd_replica_spec* spec, const double* 
 /* Advances every running replica by up to nwin windows (one launch per
  * window, replayed from a CUDA graph); replicas stop when done. */
 int clmd_ens_step(clmd_ensemble* e, int32_t nwin);
+/* Autotuner: picks the block size of each of the 4 replica-size classes
+ * (atoms <= 1024, <= 2560, <= 6144, larger) from {128, 256, 512, 1024} by
+ * timing one window per candidate on the running replicas; those 4 windows
+ * advance the simulation.  threads_out (4 entries, may be NULL) gets the
+ * choice.  Without it the classes use 128/256/512/1024 threads, or
+ * clmd_ens_config.threads for all if that is set. */
+int clmd_ens_autotune(clmd_ensemble* e, int32_t* threads_out);
 /* Per-slot results of all occupied slots (n gets the count). */
 int clmd_ens_results(clmd_ensemble* e, clmd_replica_result* out, int32_t cap, int32_t* n);
 /* Frees a finished (or unwanted) replica's pool range and slot. */
