@@ -775,6 +775,7 @@ __global__ void __launch_bounds__(NT) k_ens(Args A) {
       int* dst = (int*)&R;
       for (int k = threadIdx.x; k < (int)(sizeof(Rep) / 4); k += NT) dst[k] = src[k];
     }
+    __syncthreads();  // every word of R is written before thread 0 lays out smem from it
     if (threadIdx.x == 0) {
       int nmax = R.natom;
       const int ncell = R.ncmax * R.ncmax * R.ncmax;
