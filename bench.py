@@ -1,33 +1,42 @@
-"""Benchmark of the LJ MD step + cluster analysis on B200.
+"""Benchmark of the LJ MD step + nucleation analysis on B200.
 
-Workload (the configuration the headline metric is quoted on that fits one
-GPU): N = 262,144 atoms, rho* = 0.02, T* = 0.7, reduced LJ units, cut-off
-2.5 sigma, initial list radius 2.8 sigma (skin 0.3, adaptive, nbtim = 10),
-velocity Verlet dt* = 0.005, Stillinger clustering (1.5 sigma) with the size
-histogram every 100 steps -- the FP64 drop-in.  Seeded synthetic start:
-positions uniform with every pair >= 0.9 sigma apart, Maxwell-Boltzmann
-velocities, then stopdead(-1) and the first list/forces.
+Default workload (--workload batched): the batched nucleation ensemble the
+headline metric is quoted on -- 4096 independent replicas per GPU, N
+log-uniform in [200, 8000] (8.65 M atoms), rho* uniform in [0.01, 0.05],
+T* uniform in [0.65, 0.85], reduced LJ (rc 2.5, initial list radius 2.8,
+adaptive skin, nbtim 10), Nose-Hoover dt* = 0.005 (Q = N T* 0.25), Stillinger
+clustering every 100 steps, each replica stopping when its largest cluster
+exceeds 50 atoms (chk_nucleation, csover = 51) or after 2e5 steps; mixed
+precision (FP32 pair terms, Kahan FP32 sums, FP64 positions, velocities,
+PSI and energies).  Seeded synthetic starts (pairs >= 0.9 sigma apart,
+Maxwell-Boltzmann velocities, stopdead on the device).
 
-A bench step is one analysis cycle of main.f's loop: stoddard + the
-histogram, then 100 integrator steps.  metric = atom-steps/s.
+A bench step is one window: every running replica advances 100 steps
+(analysis + chk_nucleation first).  metric = atom-steps/s.
 
-  value   device-resident: K cycles timed with CUDA events on the engine's
-          stream; L2 (126 MB) is flushed with a 256 MB write between cycles
-          (outside the timed events).
-  e2e     the same cycles through the C ABI with host buffers: per cycle the
-          state (x, v, a) goes host->device from pinned memory, the cycle
-          runs, and the state plus the cluster histogram come back.
-  roofline  the step kernel (k_cycle, one launch = 100 steps), timed alone
-          with CUDA events; algorithmic bytes = 144 B per atom-step (read
-          and write x, v, a in FP64) against the measured copy bandwidth.
-  cpu_baseline  the serial C restatement of the reference (the oracle) on one
-          host core, on a bounded sample of the same workload.
+  value   device-resident windows, whole-job atom-steps / max-over-ranks time.
+  e2e     per window every replica's x, v go host->device from pinned memory
+          through the C ABI, the window runs, x, v come back (+ a 16-byte
+          status per replica).
+  roofline  the window kernels (k_ens, 4 size classes concurrently), CUDA
+          events inside the library; 120 algorithmic bytes per atom-step
+          (x, v FP64 and a FP32, read + written) against measured HBM.
+  fp64_dropin_same_ensemble  the FP64 drop-in (one system at a time, the
+          plain engine) timed on replicas at the size quantiles, summed over
+          the whole ensemble: the "vs FP64" of the metric.
+  cpu_baseline  the serial C restatement of the reference on one core,
+          sampled on replicas at the size quantiles.
 
---impl reference times that serial C restatement alone (the reference is
-Fortran 77 and no Fortran compiler exists on either machine), rank 0 only.
+--workload dropin: one FP64 system of N = 262,144 atoms (rho* = 0.02, T* =
+0.7, velocity Verlet, Stillinger every 100 steps), a bench step = one
+analysis cycle of 100 steps.
 
-Multi-GPU: independent replicas, one per rank (seed + rank): the path has no
-data exchange; value = all ranks' atom-steps / max-over-ranks time.
+--impl reference times the serial C restatement of the reference (the
+reference is Fortran 77 and no Fortran compiler exists on either machine) on
+the same workload, rank 0 only.
+
+Multi-GPU: independent replicas per rank (seeds offset by rank); the path has
+no data exchange; value = all ranks' atom-steps / max-over-ranks time.
 """
 import argparse
 import ctypes as C
@@ -76,9 +85,9 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per k_cycle launch from the committed ncu summary."""
-    p = os.path.join(REPO, "profiles", "k_cycle_fp64_dropin.md")
+def profiled_traffic(name="k_cycle_fp64_dropin"):
+    """DRAM bytes per launch of a kernel from its committed ncu summary."""
+    p = os.path.join(REPO, "profiles", name + ".md")
     if not os.path.exists(p):
         return None
     m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
@@ -409,26 +418,35 @@ def engine_arm(args, w):
 
 
 # ---------------------------------------------------------------------------
-# batched ensemble (configs "batched"): mixed precision vs the FP64 drop-in
+# batched ensemble: mixed precision vs the FP64 drop-in (the default workload)
 # ---------------------------------------------------------------------------
+ENSEMBLE = dict(name="batched", replicas=4096, nmin=200, nmax=8000, rho=(0.01, 0.05),
+                temp=(0.65, 0.85), csover=51, budget=200000, ftcsi=100, seed=7)
+BYTES_PER_ATOM_STEP_MIXED = 120  # x, v FP64 + a FP32, read + written
+
+
 def ensemble_specs(nrep, seed, nmin=200, nmax=8000):
     rng = np.random.default_rng(seed)
     n = np.exp(rng.uniform(np.log(nmin), np.log(nmax), nrep)).astype(int)
-    rho = rng.uniform(0.01, 0.05, nrep)
-    temp = rng.uniform(0.65, 0.85, nrep)
+    rho = rng.uniform(*ENSEMBLE["rho"], nrep)
+    temp = rng.uniform(*ENSEMBLE["temp"], nrep)
     return [(int(n[k]), float(rho[k]), float(temp[k]), seed * 100003 + k) for k in range(nrep)]
 
 
+def nh_config(n, rho, temp):
+    return clmd.lj_config(n, rho, temp, integrator=clmd.INT_NOSE, ethst="N", ftcsi=100,
+                          csover=ENSEMBLE["csover"], clwait=0, clnuctrl="X")
+
+
 def dropin_rate(n, rho, temp, seed, steps=300):
-    """atom-steps/s of the FP64 drop-in (one system per launch sequence) on
-    one replica: Nose-Hoover, Stillinger every 100 steps."""
+    """atom-steps/s of the FP64 drop-in (one system at a time) on one
+    replica: Nose-Hoover, Stillinger every 100 steps."""
     import torch
-    cfg = clmd.lj_config(n, rho, temp, integrator=clmd.INT_NOSE, ethst="N", ftcsi=100)
+    cfg = nh_config(n, rho, temp)
     st = make_state(cfg, seed, temp)
     g = start_system(cfg, st)
     s = g.scalars()
-    sumv2 = 2.0 * s.ekin
-    s.psi = (sumv2 - 3.0 * n * clmd.CIKB * cfg.att) / cfg.Q
+    s.psi = (2.0 * s.ekin - 3.0 * n * clmd.CIKB * cfg.att) / cfg.Q  # main.f:158-160
     g.set_scalars(s)
     g.run(0, 100)
     stream = torch.cuda.ExternalStream(g.stream())
@@ -442,87 +460,290 @@ def dropin_rate(n, rho, temp, seed, steps=300):
     return n * steps / (ms / 1e3)
 
 
+def oracle_rate(n, rho, temp, seed, steps=100, budget_s=4.0):
+    """atom-steps/s of the serial C restatement (all-pairs list, NH,
+    Stillinger every 100 steps) on one replica, one core."""
+    sys.path.insert(0, ORACLE)
+    import orc
+    cfg = nh_config(n, rho, temp)
+    st = make_state(cfg, seed, temp)
+    o = orc.Oracle(cfg, neighbor_mode=0)
+    o.set_state(st, scalars=orc.scalars_init(cfg))
+    o.stopdead(-1)
+    o.neighbor(0)
+    o.zero_acc()
+    o.accatom()
+    s = o.scalars()
+    s.psi = (2.0 * s.ekin - 3.0 * n * CIKB_ * cfg.att) / cfg.Q
+    o.set_scalars(s)
+    o.stoddard(-1)
+    t0 = time.perf_counter()
+    done = 0
+    chunk = 10
+    while done < steps and time.perf_counter() - t0 < budget_s:
+        o.run(done, chunk)
+        done += chunk
+    el = time.perf_counter() - t0
+    o.close()
+    return n * done / el
+
+
+CIKB_ = clmd.CIKB
+
+
+def cpu_ensemble_estimate(specs, budget_s=12.0):
+    """Serial reference algorithm on the batched workload: per-replica rates on
+    replicas at the size quantiles, summed over every replica of the ensemble
+    (the serial code runs replicas one after another)."""
+    order = sorted(range(len(specs)), key=lambda k: specs[k][0])
+    picks = [order[int(q * (len(order) - 1))] for q in (0.05, 0.35, 0.65, 0.95)]
+    rates = []
+    for k in picks:
+        n, rho, temp, sd = specs[k]
+        rates.append((n, oracle_rate(n, rho, temp, sd, budget_s=budget_s / 4)))
+    ln = np.log([r[0] for r in rates])
+    lr = np.log([r[1] for r in rates])
+    t = sum(n / float(np.exp(np.interp(np.log(n), ln, lr))) for n, _, _, _ in specs)
+    value = sum(sp[0] for sp in specs) / t  # per step of every replica
+    desc = ("serial oracle (all-pairs list, Nose-Hoover, Stillinger every 100 steps), 1 core: "
+            f"replicas of N = {[r[0] for r in rates]} run for up to 100 steps each "
+            f"({[round(r[1]) for r in rates]} atom-steps/s), rates interpolated in log N "
+            f"over all {len(specs)} replicas run one after another")
+    return value, desc
+
+
+def batched_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    specs = ensemble_specs(args.replicas, ENSEMBLE["seed"])
+    budget = min(12.0, max(2.0, 150.0 / max(1, args.warmup + args.steps)))
+    vals, desc = [], ""
+    for k in range(args.warmup + args.steps):
+        v, desc = cpu_ensemble_estimate(specs, budget_s=budget)
+        if k >= args.warmup:
+            vals.append(v)
+    value = statistics.mean(vals)
+    total = sum(sp[0] for sp in specs)
+    line = {
+        "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total * 100 / value * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": batched_config_json(args, total, [0, 0, 0, 0], 1),
+        "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": 1, "kind": "port",
+                         "sample": desc},
+        "e2e": {"value": value, "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def batched_config_json(args, total, tuned, ngpu):
+    return {"workload": f"batched-ensemble-{args.replicas}x(N=200..8000 log-uniform, "
+                        "rho*=0.01..0.05, T*=0.65..0.85)-NoseHoover-mixed",
+            "replicas_per_gpu": args.replicas, "atoms_per_gpu": total,
+            "steps_per_bench_step": 100, "clustering": "stillinger-1.5sigma every 100",
+            "stop": "largest cluster > 50 (csover=51) or 2e5 steps",
+            "threads_per_size_class": tuned,
+            "l2": "window state (~1 GB) larger than L2; no flush needed",
+            "parallelism": f"replicas x{ngpu}"}
+
+
+def mixed_force_error(e, slots, specs_by_slot, nsample=3):
+    """Relative force error of the mixed engine against the FP64 oracle on
+    the engine's own positions (normwise and worst atom above 1% of max)."""
+    sys.path.insert(0, ORACLE)
+    import orc
+    worst_n, worst_a = 0.0, 0.0
+    for k in list(slots)[:nsample]:
+        n = specs_by_slot[k][0]
+        st, _ = e.state(k)
+        rho = specs_by_slot[k][1]
+        cfg = clmd.lj_config(n, rho, 0.7)
+        o = orc.Oracle(cfg, neighbor_mode=1)
+        z0 = np.zeros(n)
+        o.set_state(clmd.State(st.x, st.y, st.z, z0, z0, z0, z0, z0, z0),
+                    scalars=orc.scalars_init(cfg))
+        o.neighbor(0)
+        o.zero_acc()
+        o.accatom()
+        r = o.get_state()
+        a = np.stack([st.ax, st.ay, st.az], 1)
+        b = np.stack([r.ax, r.ay, r.az], 1)
+        worst_n = max(worst_n, np.linalg.norm(a - b) / np.linalg.norm(b))
+        mag = np.linalg.norm(b, axis=1)
+        big = mag > 0.01 * mag.max()
+        worst_a = max(worst_a, (np.linalg.norm(a - b, axis=1)[big] / mag[big]).max())
+        o.close()
+    return worst_n, worst_a
+
+
 def batched_arm(args):
     import torch
-    torch.cuda.set_device(0)
-    clmd.set_device(0)
-    specs = ensemble_specs(args.replicas, 7)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = world > 1
+    if dist:
+        import datetime
+        import torch.distributed as td
+        torch.cuda.set_device(local)
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = local if dist else 0
+    torch.cuda.set_device(dev)
+    clmd.set_device(dev)
+
+    def barrier():
+        if dist:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def reduce(x, op):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=op)
+        return float(t.item())
+
+    specs = ensemble_specs(args.replicas, ENSEMBLE["seed"] + 1000 * rank)
     total = sum(sp[0] for sp in specs)
     e = clmd.Ensemble(clmd.ens_config(total + 1024, len(specs), precision=clmd.PREC_MIXED,
-                                      integrator=clmd.INT_NOSE, ftcsi=100,
+                                      integrator=clmd.INT_NOSE, ftcsi=ENSEMBLE["ftcsi"],
                                       threads=args.threads))
     t0 = time.perf_counter()
     slots = {}
     for n, rho, temp, sd in specs:
         box = (n / rho) ** (1.0 / 3.0)
         x, y, z, vx, vy, vz = clmd.init_random(n, (box, box, box), 0.9, temp, sd)
-        slots[e.add(n, box, temp, x, y, z, vx, vy, vz, csover=51, clwait=0,
-                    budget=200000)] = (n, rho, temp, sd)
-    log(f"admitted {len(slots)} replicas, {total} atoms in {time.perf_counter()-t0:.1f} s")
-    e.step(1)  # start sequences + first window (warm-up)
-    for _ in range(args.warmup - 1):
-        e.step(1)
+        slots[e.add(n, box, temp, x, y, z, vx, vy, vz, csover=ENSEMBLE["csover"], clwait=0,
+                    budget=ENSEMBLE["budget"])] = (n, rho, temp, sd)
+    log(f"rank {rank}: admitted {len(slots)} replicas, {total} atoms in "
+        f"{time.perf_counter()-t0:.1f} s")
+    e.step(1)  # the start sequences + a first window
     tuned = e.autotune() if args.threads == 0 else [args.threads] * 4
+    for _ in range(max(0, args.warmup - 1)):
+        e.step(1)
+
+    # ---- value: device-resident windows
     r0 = {k: v.step for k, v in e.results().items()}
-    torch.cuda.synchronize()
     l0 = e.launches()
+    clocks = Clocks(dev)
+    kern_ms, kern_bytes = [], []
+    barrier()
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
     t = time.perf_counter()
     for _ in range(args.steps):
         e.step(1)
+        ms, at = e.last_ms()
+        kern_ms.append(max(ms))
+        kern_bytes.append(sum(at) * ENSEMBLE["ftcsi"] * BYTES_PER_ATOM_STEP_MIXED)
+    ev1.record()
     torch.cuda.synchronize()
     el = time.perf_counter() - t
+    clk = clocks.stop()
+    barrier()
     res = e.results()
     atom_steps = sum(slots[k][0] * (res[k].step - r0[k]) for k in slots)
-    value = atom_steps / el
-    done = sum(1 for r in res.values() if r.done == 1)
-    # the FP64 drop-in on the same ensemble: per-replica rates on a stratified
-    # sample, total time for every replica's steps, same atom-steps
-    order = sorted(slots, key=lambda k: slots[k][0])
-    picks = [order[int(q * (len(order) - 1))] for q in np.linspace(0, 1, args.dropin_sample)]
-    rates = []
-    for k in picks:
-        n, rho, temp, sd = slots[k]
-        rates.append((n, dropin_rate(n, rho, temp, sd)))
-    ln = np.log([r[0] for r in rates])
-    lr = np.log([r[1] for r in rates])
-    t_drop = 0.0
-    for k in slots:
-        n = slots[k][0]
-        rate = float(np.exp(np.interp(np.log(n), ln, lr)))
-        t_drop += n * (res[k].step - r0[k]) / rate
-    dropin_value = atom_steps / t_drop
-    line = {
-        "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
-        "data": "synthetic (seeded)",
-        "config": {"workload": f"batched-{len(slots)}-replicas-N200-8000-NH-mixed",
-                   "replicas": len(slots), "atoms": total, "steps_per_bench_step": 100,
-                   "threads_per_size_class": tuned, "parallelism": "replicas"},
-        "fp64_dropin_same_ensemble": dropin_value,
-        "speedup_vs_fp64_dropin": value / dropin_value,
-        "dropin_sample_rates": [[n, r] for n, r in rates],
-        "nucleated": done, "gpu_launches": int(e.launches() - l0),
-    }
-    print(json.dumps(line), flush=True)
+    el_max = reduce(el, torch.distributed.ReduceOp.MAX if dist else None)
+    units = reduce(float(atom_steps), torch.distributed.ReduceOp.SUM if dist else None)
+    value = units / el_max
+    launches = e.launches() - l0
+
+    # ---- roofline: the window kernels (size classes run concurrently)
+    peak, peak_kind = measured_peaks()
+    achieved = sum(kern_bytes) / (sum(kern_ms) / 1e3) / 1e9
+
+    # ---- e2e: host buffers through the C ABI every window
+    bufs = [torch.empty(total, dtype=torch.float64).pin_memory() for _ in range(6)]
+    dp = [C.cast(b.data_ptr(), C.POINTER(C.c_double)) for b in bufs]
+    lib = e.lib
+    lib.clmd_ens_download(e.h, *dp)
+    re0 = {k: v.step for k, v in e.results().items()}
+    barrier()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        lib.clmd_ens_upload(e.h, *dp)
+        e.step(1)
+        lib.clmd_ens_download(e.h, *dp)
+    e2e_s = time.perf_counter() - t
+    barrier()
+    res = e.results()
+    e2e_units = reduce(float(sum(slots[k][0] * (res[k].step - re0[k]) for k in slots)),
+                       torch.distributed.ReduceOp.SUM if dist else None)
+    e2e_value = e2e_units / reduce(e2e_s, torch.distributed.ReduceOp.MAX if dist else None)
+    h2d = 6 * 8 * total
+    d2h = 6 * 8 * total + 16 * len(slots)
+
+    line = None
+    if rank == 0:
+        ferr_n, ferr_a = mixed_force_error(e, slots, slots)
+        order = sorted(slots, key=lambda k: slots[k][0])
+        picks = [order[int(q * (len(order) - 1))] for q in np.linspace(0, 1, args.dropin_sample)]
+        rates = [(slots[k][0], dropin_rate(*slots[k])) for k in picks]
+        ln = np.log([r[0] for r in rates])
+        lr = np.log([r[1] for r in rates])
+        t_drop = sum(slots[k][0] * 100 / float(np.exp(np.interp(np.log(slots[k][0]), ln, lr)))
+                     for k in slots)
+        dropin_value = sum(slots[k][0] * 100 for k in slots) / t_drop
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            v, desc = cpu_ensemble_estimate(specs)
+            cpu = {"value": v, "unit": "atom-steps/s", "cores": 1, "kind": "port",
+                   "sample": desc}
+        line = {
+            "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": el_max / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64", "data": "synthetic (seeded)",
+            "config": batched_config_json(args, total, tuned, world),
+            "e2e": {"value": e2e_value, "unit": "atom-steps/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": profiled_traffic("k_ens_batched"),
+                         "kernel": "k_ens (one window = 100 Nose-Hoover steps per replica; "
+                                   "4 size classes concurrently)",
+                         "algorithmic_bytes_per_atom_step": BYTES_PER_ATOM_STEP_MIXED,
+                         "kernel_ms_per_window": statistics.mean(kern_ms),
+                         "peak_kind": peak_kind},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "fp64_dropin_same_ensemble": dropin_value,
+            "speedup_vs_fp64_dropin": value / dropin_value,
+            "dropin_sample_rates": [[n, r] for n, r in rates],
+            "force_rel_err_vs_fp64": {"normwise": ferr_n, "worst_atom": ferr_a},
+            "nucleated": sum(1 for r in res.values() if r.done == 1),
+        }
+        print(json.dumps(line), flush=True)
+    e.close()
+    if dist:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
 
 
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20, help="timed analysis cycles (100 MD steps)")
+    ap.add_argument("--steps", type=int, default=10, help="timed analysis cycles (100 MD steps)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--natom", type=int, default=WORKLOAD["natom"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="dropin", choices=["dropin", "batched"])
+    ap.add_argument("--workload", default="batched", choices=["batched", "dropin"])
     ap.add_argument("--replicas", type=int, default=4096)
     ap.add_argument("--threads", type=int, default=0, help="0 = autotune")
     ap.add_argument("--dropin-sample", type=int, default=8)
     args = ap.parse_args()
     w = dict(WORKLOAD, natom=args.natom)
     if args.workload == "batched":
-        batched_arm(args)
+        if args.impl == "reference":
+            batched_reference_arm(args)
+        else:
+            batched_arm(args)
         return
     if args.impl == "reference":
         reference_arm(args, w)

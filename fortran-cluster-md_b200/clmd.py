@@ -250,6 +250,9 @@ def load(path: str = LIB_PATH):
         "clmd_ens_remove": ([P, C.c_int32], C.c_int),
         "clmd_ens_get_state": ([P, C.c_int32, d, d, d, d, d, d, d, d, d, i], C.c_int),
         "clmd_ens_fpt": ([P, C.c_int32, i, C.c_int32], C.c_int),
+        "clmd_ens_upload": ([P, d, d, d, d, d, d], C.c_int),
+        "clmd_ens_last_ms": ([P, C.POINTER(C.c_float), C.POINTER(C.c_int64)], C.c_int),
+        "clmd_ens_download": ([P, d, d, d, d, d, d], C.c_int),
         "clmd_ens_free_atoms": ([P], C.c_int64),
         "clmd_ens_launches": ([P], C.c_int64),
     }
@@ -591,6 +594,13 @@ class Ensemble:
         if st:
             raise ClmdError(st, "clmd_ens_fpt")
         return a
+
+    def last_ms(self):
+        """Device ms and atoms of the last window, per size class."""
+        ms = (C.c_float * 4)()
+        at = (C.c_int64 * 4)()
+        self.lib.clmd_ens_last_ms(self.h, ms, at)
+        return list(ms), list(at)
 
     def free_atoms(self):
         return self.lib.clmd_ens_free_atoms(self.h)

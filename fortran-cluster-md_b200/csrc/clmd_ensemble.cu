@@ -1317,3 +1317,62 @@ extern "C" int clmd_ens_fpt(clmd_ensemble* E, int32_t slot, int32_t* fpt, int32_
   for (int k = n; k < cap; k++) fpt[k] = -1;
   return CLMD_OK;
 }
+
+// slot-ordered host ranges of every occupied slot
+static void host_ranges(clmd_ensemble* E, std::vector<std::pair<long long, int>>& r) {
+  r.clear();
+  for (int s = 0; s < E->cfg.max_replicas; s++)
+    if (E->used[s]) r.push_back({E->slot_off[s], E->h_reps[s].natom});
+}
+
+extern "C" int clmd_ens_upload(clmd_ensemble* E, const double* x, const double* y,
+                               const double* z, const double* vx, const double* vy,
+                               const double* vz) {
+  if (!E) return CLMD_ERR_ARG;
+  std::lock_guard<std::mutex> lock(E->mu);
+  std::vector<std::pair<long long, int>> r;
+  host_ranges(E, r);
+  const double* src[6] = {x, y, z, vx, vy, vz};
+  double* dst[6] = {E->A.x, E->A.y, E->A.z, E->A.vx, E->A.vy, E->A.vz};
+  for (int k = 0; k < 6; k++) {
+    if (!src[k]) continue;
+    long long h = 0;
+    for (auto& q : r) {
+      ECK(cudaMemcpyAsync(dst[k] + q.first, src[k] + h, 8 * (size_t)q.second,
+                          cudaMemcpyHostToDevice, E->stream));
+      h += q.second;
+    }
+  }
+  ECK(cudaStreamSynchronize(E->stream));
+  return CLMD_OK;
+}
+
+extern "C" int clmd_ens_download(clmd_ensemble* E, double* x, double* y, double* z,
+                                 double* vx, double* vy, double* vz) {
+  if (!E) return CLMD_ERR_ARG;
+  std::lock_guard<std::mutex> lock(E->mu);
+  std::vector<std::pair<long long, int>> r;
+  host_ranges(E, r);
+  double* dst[6] = {x, y, z, vx, vy, vz};
+  const double* src[6] = {E->A.x, E->A.y, E->A.z, E->A.vx, E->A.vy, E->A.vz};
+  for (int k = 0; k < 6; k++) {
+    if (!dst[k]) continue;
+    long long h = 0;
+    for (auto& q : r) {
+      ECK(cudaMemcpyAsync(dst[k] + h, src[k] + q.first, 8 * (size_t)q.second,
+                          cudaMemcpyDeviceToHost, E->stream));
+      h += q.second;
+    }
+  }
+  ECK(cudaStreamSynchronize(E->stream));
+  return CLMD_OK;
+}
+
+extern "C" int clmd_ens_last_ms(clmd_ensemble* E, float* ms, int64_t* atoms) {
+  if (!E) return CLMD_ERR_ARG;
+  for (int c = 0; c < clmd_ensemble::kClasses; c++) {
+    if (ms) ms[c] = E->last_ms[c];
+    if (atoms) atoms[c] = E->last_atoms[c];
+  }
+  return CLMD_OK;
+}

@@ -286,9 +286,18 @@ int clmd_ens_remove(clmd_ensemble* e, int32_t slot);
 int clmd_ens_get_state(clmd_ensemble* e, int32_t slot, double* x, double* y, double* z,
                        double* vx, double* vy, double* vz, double* ax, double* ay,
                        double* az, int32_t* cl);
+/* Bulk host<->device copies of every occupied slot's x..vz, concatenated in
+ * slot order (natom of each slot, as admitted).  NULL arrays are skipped. */
+int clmd_ens_upload(clmd_ensemble* e, const double* x, const double* y, const double* z,
+                    const double* vx, const double* vy, const double* vz);
+int clmd_ens_download(clmd_ensemble* e, double* x, double* y, double* z, double* vx,
+                      double* vy, double* vz);
 /* First step at which the largest cluster reached each size 1..cap (-1 if
  * not yet). */
 int clmd_ens_fpt(clmd_ensemble* e, int32_t slot, int32_t* fpt, int32_t cap);
+/* Device time (ms, CUDA events) of the last window's launch of each of the 4
+ * size classes (-1 if the class was empty) and the atoms it advanced. */
+int clmd_ens_last_ms(clmd_ensemble* e, float* ms, int64_t* atoms);
 /* Atoms currently free in the pool. */
 int64_t clmd_ens_free_atoms(clmd_ensemble* e);
 /* Kernel launches issued so far. */
