@@ -725,6 +725,170 @@ def batched_arm(args):
         torch.distributed.destroy_process_group()
 
 
+# served solves: Poisson arrivals, continuous batching (clmd_serve)
+# ---------------------------------------------------------------------------
+SERVED = dict(rate=200.0, nmin=100, nmax=50000, rho=(0.01, 0.05), temp=(0.65, 0.85),
+              budget=(1e4, 1e6), csover=101, ftcsi=100, seed=11)
+POOL_BYTES_PER_ATOM = 9 * 8 + 3 * 8 + 192 * 4 + 6 * 4  # x..vzn, a, ELL list, int scratch
+
+
+def served_trace(arrival_s, seed):
+    """Poisson arrivals at SERVED['rate'] over [0, arrival_s): N log-uniform,
+    rho*/T* uniform, step budgets log-uniform, threshold largest cluster > 100."""
+    rng = np.random.default_rng(seed)
+    reqs, t = [], 0.0
+    while True:
+        t += rng.exponential(1.0 / SERVED["rate"])
+        if t >= arrival_s:
+            break
+        r = clmd.Request()
+        r.arrival = t
+        r.natom = int(np.exp(rng.uniform(np.log(SERVED["nmin"]), np.log(SERVED["nmax"]))))
+        r.rho = float(rng.uniform(*SERVED["rho"]))
+        r.temp = float(rng.uniform(*SERVED["temp"]))
+        r.budget = int(np.exp(rng.uniform(*np.log(SERVED["budget"]))))
+        r.csover = SERVED["csover"]
+        r.seed = seed * 1000003 + len(reqs)
+        reqs.append(r)
+    return reqs
+
+
+def served_config_json(args, nreq, pool, ngpu):
+    return {"workload": f"served-poisson-{SERVED['rate']:.0f}req/s-for-{args.arrival_seconds}s"
+                        "(N=100..50000 log-uniform, rho*=0.01..0.05, T*=0.65..0.85, "
+                        "budget 1e4..1e6 log-uniform)-NoseHoover-mixed",
+            "requests_per_gpu": nreq, "pool_atoms": pool,
+            "admission": "free HBM: atom pool sized from cudaMemGetInfo",
+            "stop": "largest cluster > 100 (csover=101) or budget",
+            "window_steps": SERVED["ftcsi"], "max_seconds": args.serve_seconds,
+            "l2": "no flush; resident state grows past L2 as requests arrive",
+            "parallelism": f"independent traces x{ngpu}"}
+
+
+def served_arm(args):
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = world > 1
+    if dist:
+        import datetime
+        import torch.distributed as td
+        torch.cuda.set_device(local)
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dev = local if dist else 0
+    torch.cuda.set_device(dev)
+    clmd.set_device(dev)
+    free, _ = torch.cuda.mem_get_info(dev)
+    pool = int(min(args.pool_fraction * free / POOL_BYTES_PER_ATOM, 2**31 - 1))
+    reqs = served_trace(args.arrival_seconds, SERVED["seed"] + 1000 * rank)
+    e = clmd.Ensemble(clmd.ens_config(pool, 16384, precision=clmd.PREC_MIXED,
+                                      integrator=clmd.INT_NOSE, ftcsi=SERVED["ftcsi"],
+                                      threads=args.threads or 0))
+    # block sizes per size class from a short tuning trace (not timed)
+    warm = served_trace(0.25, SERVED["seed"] + 999 + 1000 * rank)
+    for r in warm:
+        r.arrival = 0.0
+        r.budget = 400
+    e.serve(warm, 30.0)
+    if dist:
+        torch.distributed.barrier()
+    clocks = Clocks(dev)
+    l0 = e.launches()
+    clocks.start()
+    out, st = e.serve(reqs, args.serve_seconds)
+    clk = clocks.stop()
+    launches = e.launches() - l0
+
+    def red(x, op):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=op)
+        return float(t.item())
+
+    SUM = torch.distributed.ReduceOp.SUM if dist else None
+    MAX = torch.distributed.ReduceOp.MAX if dist else None
+    wall = red(st.wall, MAX)
+    units = red(st.atom_steps, SUM)
+    value = units / wall
+    if rank == 0:
+        lat = np.array([o.finished - o.arrival for o in out if o.done in (1, 2)])
+        nuc = np.array([o.finished - o.arrival for o in out if o.done == 1])
+        wait = np.array([o.admitted - o.arrival for o in out if o.admitted >= 0])
+        unfinished = sum(1 for o in out if o.done == 0)
+
+        def pct(a, q):
+            return float(np.percentile(a, q)) if len(a) else None
+        # a percentile over all requests is a lower bound while requests past
+        # it are still running when the window closes
+        censored_p99 = unfinished > 0.01 * len(out)
+        admitted_atoms = sum(o.natom for o in out if o.admitted >= 0)
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            specs = [(r.natom, r.rho, r.temp, r.seed) for r in reqs]
+            v, desc = cpu_ensemble_estimate(specs)
+            cpu = {"value": v, "unit": "atom-steps/s", "cores": 1, "kind": "port",
+                   "sample": desc}
+        line = {
+            "metric": "atom-steps/s (served)", "value": value, "unit": "atom-steps/s",
+            "n_gpus": world, "steps": st.windows, "warmup": 1,
+            "ms_per_step": wall / max(1, st.windows) * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic (seeded Poisson trace)",
+            "config": served_config_json(args, len(reqs), pool, world),
+            "e2e": {"value": value, "unit": "atom-steps/s",
+                    "h2d_bytes_per_step": 48 * admitted_atoms / max(1, st.windows),
+                    "d2h_bytes_per_step": 16 * st.peak_resident,
+                    "note": "the served loop is end to end: host start states in, "
+                            "per-window status out, wall clock"},
+            "latency_s": {"p50": pct(lat, 50), "p99": pct(lat, 99),
+                          "p99_is_lower_bound": censored_p99,
+                          "time_to_nucleation_p50": pct(nuc, 50),
+                          "time_to_nucleation_p99": pct(nuc, 99),
+                          "admission_wait_p50": pct(wait, 50), "admission_wait_p99": pct(wait, 99)},
+            "requests": {"arrived": len(reqs), "admitted": st.admitted,
+                         "completed": st.completed, "nucleated": int(len(nuc)),
+                         "unfinished": unfinished, "peak_resident": st.peak_resident,
+                         "peak_atoms": int(st.peak_atoms)},
+            "gpu_launches": int(launches),
+            "cpu_baseline": cpu,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    e.close()
+    if dist:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def served_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    reqs = served_trace(args.arrival_seconds, SERVED["seed"])
+    specs = [(r.natom, r.rho, r.temp, r.seed) for r in reqs]
+    vals, desc = [], ""
+    for k in range(max(1, args.warmup // 3) + 1):
+        v, desc = cpu_ensemble_estimate(specs)
+        if k > 0:
+            vals.append(v)
+    value = statistics.mean(vals)
+    line = {
+        "metric": "atom-steps/s (served)", "value": value, "unit": "atom-steps/s",
+        "impl": "reference", "n_gpus": args.gpus, "steps": len(vals), "warmup": 1,
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded Poisson trace)",
+        "config": served_config_json(args, len(reqs), 0, 1),
+        "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": 1, "kind": "port",
+                         "sample": desc},
+        "e2e": {"value": value, "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -733,12 +897,24 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--natom", type=int, default=WORKLOAD["natom"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="batched", choices=["batched", "dropin"])
+    ap.add_argument("--workload", default="batched", choices=["batched", "dropin", "served"])
+    ap.add_argument("--arrival-seconds", type=float, default=1.0,
+                    help="served: length of the Poisson arrival window")
+    ap.add_argument("--serve-seconds", type=float, default=60.0,
+                    help="served: wall-clock cap of the served loop")
+    ap.add_argument("--pool-fraction", type=float, default=0.5,
+                    help="served: share of free HBM given to the atom pool")
     ap.add_argument("--replicas", type=int, default=4096)
     ap.add_argument("--threads", type=int, default=0, help="0 = autotune")
     ap.add_argument("--dropin-sample", type=int, default=8)
     args = ap.parse_args()
     w = dict(WORKLOAD, natom=args.natom)
+    if args.workload == "served":
+        if args.impl == "reference":
+            served_reference_arm(args)
+        else:
+            served_arm(args)
+        return
     if args.workload == "batched":
         if args.impl == "reference":
             batched_reference_arm(args)

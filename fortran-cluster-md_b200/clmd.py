@@ -177,6 +177,36 @@ class ReplicaResult(C.Structure):
     ]
 
 
+class Request(C.Structure):
+    """clmd_request (include/clmd.h)."""
+
+    _fields_ = [
+        ("arrival", C.c_double), ("rho", C.c_double), ("temp", C.c_double),
+        ("seed", C.c_uint64), ("natom", C.c_int32), ("budget", C.c_int32),
+        ("csover", C.c_int32), ("pad", C.c_int32),
+    ]
+
+
+class RequestResult(C.Structure):
+    """clmd_request_result (include/clmd.h)."""
+
+    _fields_ = [
+        ("arrival", C.c_double), ("admitted", C.c_double), ("finished", C.c_double),
+        ("natom", C.c_int32), ("steps", C.c_int32), ("done", C.c_int32), ("clbrkt", C.c_int32),
+        ("status", C.c_int32), ("pad", C.c_int32),
+    ]
+
+
+class ServeStats(C.Structure):
+    """clmd_serve_stats (include/clmd.h)."""
+
+    _fields_ = [
+        ("wall", C.c_double), ("atom_steps", C.c_double), ("windows", C.c_int32),
+        ("admitted", C.c_int32), ("completed", C.c_int32), ("peak_resident", C.c_int32),
+        ("peak_atoms", C.c_int64),
+    ]
+
+
 # (name, dtype, length kind) of every cluster output: "N" or "N1" (= N+1)
 CLUSTER_FIELDS = [
     ("cl", np.int32, "N"), ("cs", np.int32, "N"), ("csi", np.int32, "N1"),
@@ -245,9 +275,13 @@ def load(path: str = LIB_PATH):
         "clmd_ens_destroy": ([P], C.c_int),
         "clmd_ens_add": ([P, C.POINTER(ReplicaSpec), d, d, d, d, d, d, i], C.c_int),
         "clmd_ens_step": ([P, C.c_int32], C.c_int),
+        "clmd_ens_step_timed": ([P, C.c_float], C.c_int),
         "clmd_ens_autotune": ([P, i], C.c_int),
         "clmd_ens_results": ([P, C.POINTER(ReplicaResult), C.c_int32, i], C.c_int),
+        "clmd_ens_poll": ([P, C.POINTER(ReplicaResult), C.c_int32, i], C.c_int),
         "clmd_ens_remove": ([P, C.c_int32], C.c_int),
+        "clmd_serve": ([P, C.POINTER(Request), C.c_int32, C.c_double,
+                        C.POINTER(RequestResult), C.POINTER(ServeStats)], C.c_int),
         "clmd_ens_get_state": ([P, C.c_int32, d, d, d, d, d, d, d, d, d, i], C.c_int),
         "clmd_ens_fpt": ([P, C.c_int32, i, C.c_int32], C.c_int),
         "clmd_ens_upload": ([P, d, d, d, d, d, d], C.c_int),
@@ -555,6 +589,13 @@ class Ensemble:
         if st:
             raise ClmdError(st, "clmd_ens_step")
 
+    def step_timed(self, min_ms):
+        """Balanced step: each replica runs as many windows as fit in about
+        max(min_ms, the longest one-window time) of device time."""
+        st = self.lib.clmd_ens_step_timed(self.h, min_ms)
+        if st:
+            raise ClmdError(st, "clmd_ens_step_timed")
+
     def autotune(self):
         """Block size per replica-size class, picked by timing (4 windows)."""
         out = (C.c_int32 * 4)()
@@ -571,6 +612,28 @@ class Ensemble:
         if st:
             raise ClmdError(st, "clmd_ens_results")
         return {out[k].slot: out[k] for k in range(n.value)}
+
+    def poll(self):
+        """Cheap per-window status (full record only for finished replicas)."""
+        cap = len(self.natom) + 1
+        out = (ReplicaResult * cap)()
+        n = C.c_int32(0)
+        st = self.lib.clmd_ens_poll(self.h, out, cap, C.byref(n))
+        if st:
+            raise ClmdError(st, "clmd_ens_poll")
+        return {out[k].slot: out[k] for k in range(n.value)}
+
+    def serve(self, requests, max_seconds):
+        """Runs a request trace (a sequence of Request) through the served
+        loop; returns (list of RequestResult, ServeStats)."""
+        n = len(requests)
+        reqs = (Request * max(n, 1))(*requests)
+        out = (RequestResult * max(n, 1))()
+        stats = ServeStats()
+        st = self.lib.clmd_serve(self.h, reqs, n, max_seconds, out, C.byref(stats))
+        if st:
+            raise ClmdError(st, "clmd_serve")
+        return [out[k] for k in range(n)], stats
 
     def remove(self, slot):
         st = self.lib.clmd_ens_remove(self.h, slot)

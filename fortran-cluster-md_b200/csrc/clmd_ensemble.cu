@@ -57,12 +57,14 @@ struct Args {
   int *list, *rlen, *sorted, *cellid, *parent, *cs, *cl, *fpt;
   Rep* reps;
   const int* items;
+  const int* iwin;  // windows per item (nullptr: nwin for every item)
   int nitems;
   int* ctr;
   double rc, atskin, dt;
   int nbtim, ftcsi, lstride, integrator, nwin;
   int ncmax;  // cells per dimension this launch's shared memory holds
   int4* summary;  // per slot: done, status, step, maxcs
+  float* wtime;   // per slot: device ms per MD step in its last launch (one CTA)
 };
 
 __device__ __forceinline__ double wsum(double v) {
@@ -136,6 +138,7 @@ struct Cta {
   double cf, rs2;
   int flag;
   int rep;  // slot of the replica being run
+  int nwin;  // windows this replica runs in this launch
 };
 
 template <bool SM>
@@ -604,7 +607,7 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
     }
     __syncthreads();
   }
-  for (int w = 0; w < A.nwin; w++) {
+  for (int w = 0; w < C.nwin; w++) {
     if (R.done || R.status) break;
     // wrt-csi.f:27 + chk_nucleation (main.f:157-161) at an analysis step
     if (A.ftcsi > 0 && R.step % A.ftcsi == 0 && R.cstep != R.step) {
@@ -707,12 +710,18 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
             double V[3] = {A.vx[off + i], A.vy[off + i], A.vz[off + i]};
             double a3[3] = {ax, ay, az};
             double* vn[3] = {A.vxn, A.vyn, A.vzn};
+            // int-verlet-nh-mav.f:117-147 rounded term by term: with fused
+            // multiply-adds the residual b never reaches exactly zero, the
+            // sweep keeps moving a near-zero component by ~1e-18 and the
+            // relative test below then fails where the reference converges
 #pragma unroll
             for (int d = 0; d < 3; d++) {
               double vo = vn[d][off + i];
-              double b = -dth * (a3[d] - pso * vo) - (V[d] - vo);
-              double nx = vo + (b + dth * vo * delps) / di;
-              if (fabs((nx - vo) / nx) > err) nr = 1;
+              double b = __dsub_rn(__dmul_rn(-dth, __dsub_rn(a3[d], __dmul_rn(pso, vo))),
+                                   __dsub_rn(V[d], vo));
+              double nx =
+                  __dadd_rn(vo, __ddiv_rn(__dadd_rn(b, __dmul_rn(__dmul_rn(dth, vo), delps)), di));
+              if (fabs(__ddiv_rn(__dsub_rn(nx, vo), nx)) > err) nr = 1;
               vn[d][off + i] = nx;
               s2 += nx * nx;
             }
@@ -742,6 +751,16 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
         }
       }
       if (tid == 0) R.step = step + 1;
+      __syncthreads();
+    }
+    // a spent budget ends the replica in this window, after the analysis due
+    // at its last step, rather than at the start of the next window
+    const bool spent = R.step >= R.budget && !R.done && !R.status;
+    __syncthreads();
+    if (spent) {
+      if (A.ftcsi > 0 && R.step % A.ftcsi == 0 && R.cstep != R.step)
+        analysis<NT, SM>(R, C, A, P, R.step);
+      if (tid == 0 && !R.done) R.done = 2;
       __syncthreads();
     }
   }
@@ -788,7 +807,19 @@ __global__ void __launch_bounds__(NT) k_ens(Args A) {
       C.sz = SM ? p + 2 * nmax : nullptr;
     }
     __syncthreads();
+    unsigned long long t0 = 0;
+    const int step0 = R.step;
+    if (threadIdx.x == 0) {
+      C.nwin = A.iwin ? A.iwin[it] : A.nwin;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    }
+    __syncthreads();
     if (!R.done && !R.status) run_window<NT, SM, MIXED>(R, C, A);
+    if (threadIdx.x == 0 && R.step > step0) {
+      unsigned long long t1;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
+      A.wtime[r] = (float)((double)(t1 - t0) * 1e-6 / (double)(R.step - step0));
+    }
     {
       const int* src = (const int*)&R;
       int* dst = (int*)(A.reps + r);
@@ -822,6 +853,9 @@ struct clmd_ensemble {
   int* d_items = nullptr;
   int* d_ctr = nullptr;
   int* h_items = nullptr;  // pinned
+  int* d_iwin = nullptr;   // windows per item (balanced launches)
+  int* h_iwin = nullptr;   // pinned
+  float* h_wtime = nullptr;  // pinned copy of A.wtime
   int4* h_summary = nullptr;  // pinned copy of A.summary
   bool reps_stale = false;    // h_reps older than the device records
   // size classes: each has its own block size, shared-memory budget, stream
@@ -879,7 +913,10 @@ extern "C" int clmd_ens_create(const clmd_ens_config* cfg, clmd_ensemble** out) 
   }
   clmd_ensemble* E = new clmd_ensemble();
   E->cfg = *cfg;
-  if (E->cfg.list_stride <= 0) E->cfg.list_stride = 96;
+  // a full list row holds every neighbour within the list radius: ~5 in the
+  // vapour, ~130 inside a liquid droplet (rho* 0.85, radius 3.3); the stride
+  // only sizes the allocation, rebuilds write the rows' real lengths
+  if (E->cfg.list_stride <= 0) E->cfg.list_stride = 192;
   if (E->cfg.threads <= 0) E->cfg.threads = 256;
   E->threads = E->cfg.threads;
   ECK(cudaGetDevice(&E->dev));
@@ -922,6 +959,12 @@ extern "C" int clmd_ens_create(const clmd_ens_config* cfg, clmd_ensemble** out) 
   ECK(cudaMallocHost(&E->h_reps, sizeof(Rep) * R));
   memset(E->h_reps, 0, sizeof(Rep) * R);
   ECK(cudaMalloc(&E->d_items, sizeof(int) * R));
+  ECK(cudaMalloc(&E->d_iwin, sizeof(int) * R));
+  ECK(cudaMallocHost(&E->h_iwin, sizeof(int) * R));
+  ECK(cudaMalloc(&A.wtime, sizeof(float) * R));
+  ECK(cudaMemset(A.wtime, 0, sizeof(float) * R));
+  ECK(cudaMallocHost(&E->h_wtime, sizeof(float) * R));
+  memset(E->h_wtime, 0, sizeof(float) * R);
   ECK(cudaMalloc(&E->d_ctr, sizeof(int) * 16));
   ECK(cudaMallocHost(&E->h_items, sizeof(int) * R));
   A.items = E->d_items;
@@ -946,11 +989,13 @@ extern "C" int clmd_ens_destroy(clmd_ensemble* E) {
   Args& A = E->A;
   void* ps[] = {A.x, A.y, A.z, A.vx, A.vy, A.vz, A.vxn, A.vyn, A.vzn, A.a, A.list, A.rlen,
                 A.sorted, A.cellid, A.parent, A.cs, A.cl, A.reps, A.fpt, A.summary,
-                E->d_items, E->d_ctr};
+                E->d_items, E->d_ctr, E->d_iwin, A.wtime};
   for (void* p : ps)
     if (p) cudaFree(p);
   if (E->h_reps) cudaFreeHost(E->h_reps);
   if (E->h_items) cudaFreeHost(E->h_items);
+  if (E->h_iwin) cudaFreeHost(E->h_iwin);
+  if (E->h_wtime) cudaFreeHost(E->h_wtime);
   if (E->h_summary) cudaFreeHost(E->h_summary);
   if (E->stream) cudaStreamDestroy(E->stream);
   for (int c = 0; c < clmd_ensemble::kClasses; c++) {
@@ -1074,8 +1119,7 @@ extern "C" int clmd_ens_remove(clmd_ensemble* E, int32_t slot) {
   if (!E || slot < 0 || slot >= E->cfg.max_replicas || !E->used[slot]) return CLMD_ERR_ARG;
   std::lock_guard<std::mutex> lock(E->mu);
   ECK(cudaStreamSynchronize(E->stream));
-  int rs = refresh_reps(E);
-  if (rs) return rs;
+  // natom is the admission value on the host whether or not h_reps is stale
   pool_free(E, E->slot_off[slot], E->h_reps[slot].natom);
   E->used[slot] = 0;
   E->slot_off[slot] = -1;
@@ -1108,7 +1152,7 @@ static EnsKernel kernel_for(int nt, bool sm, bool mixed) {
 // one launch of one size class: every listed replica advances by nwin
 // windows; items[] is the class's slice of the device item list
 static int launch_class(clmd_ensemble* E, int c, int item0, int nitems, const int* slots,
-                        int nwin, int nt) {
+                        int nwin, int nt, bool balanced) {
   if (nitems == 0) return CLMD_OK;
   const bool mixed = E->cfg.precision == CLMD_PREC_MIXED;
   // positions stay in shared memory if every replica of the class fits
@@ -1134,6 +1178,7 @@ static int launch_class(clmd_ensemble* E, int c, int item0, int nitems, const in
   ECK(cudaMemsetAsync(E->d_ctr + c, 0, sizeof(int), st));
   Args A = E->A;
   A.items = E->d_items + item0;
+  A.iwin = balanced ? E->d_iwin + item0 : nullptr;
   A.ctr = E->d_ctr + c;
   A.nitems = nitems;
   A.nwin = nwin;
@@ -1147,7 +1192,11 @@ static int launch_class(clmd_ensemble* E, int c, int item0, int nitems, const in
 
 // all running replicas, split by size class, each class largest first; the
 // classes run concurrently on their own streams
-static int launch_all(clmd_ensemble* E, int nwin, const int* threads) {
+// min_ms > 0: balanced launch -- replica i runs nwin * k_i windows, k_i =
+// max(1, floor(T / t_i)), t_i its measured one-window device time and T =
+// max(min_ms, max t_i), so that every CTA stays busy about as long as the
+// longest replica's window (a replica not yet timed runs nwin windows)
+static int launch_all(clmd_ensemble* E, int nwin, const int* threads, float min_ms = 0.0f) {
   std::vector<int> cls[clmd_ensemble::kClasses];
   int nmax[clmd_ensemble::kClasses] = {};
   for (int s = 0; s < E->cfg.max_replicas; s++)
@@ -1167,6 +1216,20 @@ static int launch_all(clmd_ensemble* E, int nwin, const int* threads) {
     memcpy(E->h_items + total, cls[c].data(), sizeof(int) * cls[c].size());
     total += (int)cls[c].size();
   }
+  const bool balanced = min_ms > 0.0f;
+  if (balanced && total > 0) {
+    const int wsteps = E->cfg.ftcsi > 0 ? E->cfg.ftcsi : 1;
+    float T = min_ms;
+    for (int k = 0; k < total; k++) T = std::max(T, E->h_wtime[E->h_items[k]] * wsteps);
+    for (int k = 0; k < total; k++) {
+      const float t = E->h_wtime[E->h_items[k]] * wsteps;
+      long long w = t > 0.0f ? (long long)(T / t) : 1;
+      w = std::max(1LL, std::min(w, 4096LL)) * nwin;
+      E->h_iwin[k] = (int)std::min(w, (long long)1 << 24);
+    }
+    ECK(cudaMemcpyAsync(E->d_iwin, E->h_iwin, sizeof(int) * total, cudaMemcpyHostToDevice,
+                        E->stream));
+  }
   if (total == 0) return CLMD_OK;
   ECK(cudaMemcpyAsync(E->d_items, E->h_items, sizeof(int) * total, cudaMemcpyHostToDevice,
                       E->stream));
@@ -1177,7 +1240,8 @@ static int launch_all(clmd_ensemble* E, int nwin, const int* threads) {
     for (int s : cls[c]) E->last_atoms[c] += E->h_reps[s].natom;
     if (!cls[c].empty()) {
       ECK(cudaStreamWaitEvent(E->cstream[c], E->evj, 0));
-      int st = launch_class(E, c, off, (int)cls[c].size(), cls[c].data(), nwin, threads[c]);
+      int st = launch_class(E, c, off, (int)cls[c].size(), cls[c].data(), nwin, threads[c],
+                            balanced);
       if (st) return st;
     }
     off += (int)cls[c].size();
@@ -1189,6 +1253,8 @@ static int launch_all(clmd_ensemble* E, int nwin, const int* threads) {
     }
     ECK(cudaStreamWaitEvent(E->stream, E->ev1[c], 0));
   }
+  ECK(cudaMemcpyAsync(E->h_wtime, E->A.wtime, sizeof(float) * E->cfg.max_replicas,
+                      cudaMemcpyDeviceToHost, E->stream));
   ECK(cudaMemcpyAsync(E->h_summary, E->A.summary, sizeof(int4) * E->cfg.max_replicas,
                       cudaMemcpyDeviceToHost, E->stream));
   ECK(cudaStreamSynchronize(E->stream));
@@ -1234,6 +1300,12 @@ extern "C" int clmd_ens_step(clmd_ensemble* E, int32_t nwin) {
   return launch_all(E, nwin, E->cls_threads);
 }
 
+extern "C" int clmd_ens_step_timed(clmd_ensemble* E, float min_ms) {
+  if (!E || !(min_ms > 0.0f)) return CLMD_ERR_ARG;
+  std::lock_guard<std::mutex> lock(E->mu);
+  return launch_all(E, 1, E->cls_threads, min_ms);
+}
+
 extern "C" int clmd_ens_autotune(clmd_ensemble* E, int32_t* threads_out) {
   if (!E) return CLMD_ERR_ARG;
   std::lock_guard<std::mutex> lock(E->mu);
@@ -1241,6 +1313,21 @@ extern "C" int clmd_ens_autotune(clmd_ensemble* E, int32_t* threads_out) {
   if (threads_out)
     for (int c = 0; c < clmd_ensemble::kClasses; c++) threads_out[c] = E->cls_threads[c];
   return st;
+}
+
+static void fill_result(const Rep& R, int s, clmd_replica_result& o) {
+  o.ekin = R.ekin;
+  o.epot = R.epot;
+  o.psi = R.psi;
+  o.s = R.s;
+  o.slot = s;
+  o.natom = R.natom;
+  o.step = R.step;
+  o.status = R.status;
+  o.done = R.done;
+  o.clbrkt = R.clbrkt;
+  o.maxcs = R.maxcs;
+  o.nrebuild = R.nrebuild;
 }
 
 extern "C" int clmd_ens_results(clmd_ensemble* E, clmd_replica_result* out, int32_t cap,
@@ -1253,20 +1340,41 @@ extern "C" int clmd_ens_results(clmd_ensemble* E, clmd_replica_result* out, int3
   for (int s = 0; s < E->cfg.max_replicas; s++) {
     if (!E->used[s]) continue;
     if (out && k < cap) {
-      const Rep& R = E->h_reps[s];
+      fill_result(E->h_reps[s], s, out[k]);
+    }
+    k++;
+  }
+  *n = k;
+  return CLMD_OK;
+}
+
+extern "C" int clmd_ens_poll(clmd_ensemble* E, clmd_replica_result* out, int32_t cap,
+                             int32_t* n) {
+  if (!E || !n) return CLMD_ERR_ARG;
+  std::lock_guard<std::mutex> lock(E->mu);
+  int k = 0;
+  for (int s = 0; s < E->cfg.max_replicas; s++) {
+    if (!E->used[s]) continue;
+    if (out && k < cap) {
+      const int4 q = E->h_summary[s];
       clmd_replica_result& o = out[k];
-      o.ekin = R.ekin;
-      o.epot = R.epot;
-      o.psi = R.psi;
-      o.s = R.s;
-      o.slot = s;
-      o.natom = R.natom;
-      o.step = R.step;
-      o.status = R.status;
-      o.done = R.done;
-      o.clbrkt = R.clbrkt;
-      o.maxcs = R.maxcs;
-      o.nrebuild = R.nrebuild;
+      if (q.x || q.y) {  // finished: its full record, one slot's copy
+        if (E->reps_stale) {
+          Rep R;
+          ECK(cudaMemcpyAsync(&R, E->A.reps + s, sizeof(Rep), cudaMemcpyDeviceToHost,
+                              E->stream));
+          ECK(cudaStreamSynchronize(E->stream));
+          fill_result(R, s, o);
+        } else {
+          fill_result(E->h_reps[s], s, o);
+        }
+      } else {
+        memset(&o, 0, sizeof(o));
+        o.slot = s;
+        o.natom = E->h_reps[s].natom;
+        o.step = q.z;
+        o.maxcs = q.w;
+      }
     }
     k++;
   }

@@ -119,6 +119,12 @@ extern "C" int64_t clmd_struct_size(int which) {
     case 0: return (int64_t)sizeof(clmd_config);
     case 1: return (int64_t)sizeof(clmd_scalars);
     case 2: return (int64_t)sizeof(clmd_cluster_view);
+    case 3: return (int64_t)sizeof(clmd_ens_config);
+    case 4: return (int64_t)sizeof(clmd_replica_spec);
+    case 5: return (int64_t)sizeof(clmd_replica_result);
+    case 6: return (int64_t)sizeof(clmd_request);
+    case 7: return (int64_t)sizeof(clmd_request_result);
+    case 8: return (int64_t)sizeof(clmd_serve_stats);
     default: return -1;
   }
 }

@@ -226,7 +226,7 @@ typedef struct clmd_ens_config {
   double rc, rskin, atskin, dt;  /* sigma units: cut-off, initial list radius, cluster radius */
   int64_t max_atoms;             /* atom pool (the admission budget) */
   int32_t max_replicas;
-  int32_t list_stride;           /* neighbour slots per atom; 0 = autotune */
+  int32_t list_stride;           /* neighbour slots per atom (full rows); 0 = 192 */
   int32_t precision;             /* CLMD_PREC_MIXED or CLMD_PREC_FP64 */
   int32_t integrator;            /* CLMD_INT_VERLET or CLMD_INT_NOSE */
   int32_t ftcsi;                 /* steps per window (between cluster analyses) */
@@ -270,6 +270,14 @@ int clmd_ens_add(clmd_ensemble* e, const clmd_replica_spec* spec, const double* 
 /* Advances every running replica by up to nwin windows (one launch per
  * window, replayed from a CUDA graph); replicas stop when done. */
 int clmd_ens_step(clmd_ensemble* e, int32_t nwin);
+/* Balanced step for mixed sizes: every running replica advances by k >= 1
+ * windows, k chosen per replica so that each runs for about the same device
+ * time T = max(min_ms, the longest one-window time among them), from window
+ * times the kernel measured per replica in earlier launches (a replica not
+ * yet timed runs one window).  Small replicas then do not idle while the
+ * largest finishes its window.  Trajectories are those of clmd_ens_step:
+ * only how many windows one launch covers differs. */
+int clmd_ens_step_timed(clmd_ensemble* e, float min_ms);
 /* Autotuner: picks the block size of each of the 4 replica-size classes
  * (atoms <= 1024, <= 2560, <= 6144, larger) from {128, 256, 512, 1024} by
  * timing one window per candidate on the running replicas; those 4 windows
@@ -279,6 +287,11 @@ int clmd_ens_step(clmd_ensemble* e, int32_t nwin);
 int clmd_ens_autotune(clmd_ensemble* e, int32_t* threads_out);
 /* Per-slot results of all occupied slots (n gets the count). */
 int clmd_ens_results(clmd_ensemble* e, clmd_replica_result* out, int32_t cap, int32_t* n);
+/* Per-window status without the full table copy: for every occupied slot
+ * slot, natom, step, status, done and maxcs from the summary the last step
+ * call read back; the rest of the record (energies, clbrkt, nrebuild) only
+ * for replicas that finished (done != 0 or status != 0), zero otherwise. */
+int clmd_ens_poll(clmd_ensemble* e, clmd_replica_result* out, int32_t cap, int32_t* n);
 /* Frees a finished (or unwanted) replica's pool range and slot. */
 int clmd_ens_remove(clmd_ensemble* e, int32_t slot);
 /* Copies one replica's state (x..vz, ax..az, cluster labels cl, 1-based) out;
@@ -303,6 +316,44 @@ int64_t clmd_ens_free_atoms(clmd_ensemble* e);
 /* Kernel launches issued so far. */
 int64_t clmd_ens_launches(clmd_ensemble* e);
 
+/* ---- served mode: continuous batching over a request trace ---------------
+ * Requests arrive at given times (seconds after the call starts).  At every
+ * window boundary the loop admits, in arrival order, each arrived request
+ * whose start state is ready and whose atoms fit the free pool (the pool is
+ * the admission budget, sized from free device memory by the caller), runs
+ * one window for everything resident, and retires replicas whose largest
+ * cluster crossed csover (chk_nucleation) or whose budget is spent.  Start
+ * states (uniform positions, pairs >= 0.9 apart, Maxwell-Boltzmann) are
+ * generated ahead of admission by a pool of host threads. */
+typedef struct clmd_request {
+  double arrival;    /* seconds after the start of clmd_serve */
+  double rho, temp;  /* reduced density and temperature */
+  uint64_t seed;
+  int32_t natom, budget, csover, pad;
+} clmd_request;
+
+typedef struct clmd_request_result {
+  double arrival, admitted, finished; /* seconds; admitted/finished < 0: never */
+  int32_t natom, steps;               /* steps run */
+  int32_t done;                       /* 1 nucleated, 2 budget spent, 0 not finished
+                                         or failed (status) */
+  int32_t clbrkt;                     /* step the >= csover cluster was first seen */
+  int32_t status;                     /* CLMD_OK, or the error that ended the replica */
+  int32_t pad;
+} clmd_request_result;
+
+typedef struct clmd_serve_stats {
+  double wall;        /* seconds */
+  double atom_steps;  /* every replica's steps x atoms */
+  int32_t windows, admitted, completed, peak_resident;
+  int64_t peak_atoms;
+} clmd_serve_stats;
+
+/* Runs the trace until every request finished or max_seconds passed.
+ * out[nreq] gets per-request timings. */
+int clmd_serve(clmd_ensemble* e, const clmd_request* reqs, int32_t nreq, double max_seconds,
+               clmd_request_result* out, clmd_serve_stats* stats);
+
 /* No counterpart in the reference: the Stillinger analysis (what stoddard()
  * of stoddard-pbc-n-m.f computes: labels cl, sizes cs, histogram csi) for
  * callers that cannot let the library allocate device memory -- hosts that
@@ -325,8 +376,10 @@ int clmd_stoddard_noalloc(int32_t natom, const double* x, const double* y, const
                           int32_t* cs, int32_t* csi, void* stream);
 
 const char* clmd_status_string(int status);
-/* sizeof of the ABI structs (0 config, 1 scalars, 2 cluster view), so that
- * bindings in other languages can check their layout. */
+/* sizeof of the ABI structs (0 config, 1 scalars, 2 cluster view, 3 ensemble
+ * config, 4 replica spec, 5 replica result, 6 request, 7 request result,
+ * 8 serve stats), so that bindings in other languages can check their
+ * layout. */
 int64_t clmd_struct_size(int which);
 /* Last status returned by any clmd_* or F77 entry point of this process. */
 int32_t clmd_last_status(void);

@@ -53,6 +53,12 @@ def test_struct_layouts_match_bindings():
     assert lib.clmd_struct_size(0) == C.sizeof(clmd.Config)
     assert lib.clmd_struct_size(1) == C.sizeof(clmd.Scalars)
     assert lib.clmd_struct_size(2) == C.sizeof(clmd.ClusterView)
+    assert lib.clmd_struct_size(3) == C.sizeof(clmd.EnsConfig)
+    assert lib.clmd_struct_size(4) == C.sizeof(clmd.ReplicaSpec)
+    assert lib.clmd_struct_size(5) == C.sizeof(clmd.ReplicaResult)
+    assert lib.clmd_struct_size(6) == C.sizeof(clmd.Request)
+    assert lib.clmd_struct_size(7) == C.sizeof(clmd.RequestResult)
+    assert lib.clmd_struct_size(8) == C.sizeof(clmd.ServeStats)
 
 
 def test_no_device_is_reported_not_faked():

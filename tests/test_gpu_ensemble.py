@@ -120,3 +120,120 @@ def test_admission_by_pool_and_removal(gpu):
     assert s2 is not None
     e.step(1)
     assert e.results()[s2].step == 10
+
+
+def served_requests():
+    """A small trace: staggered arrivals, sizes across the size classes,
+    budgets that are and are not multiples of the window, low thresholds so
+    that some replicas nucleate."""
+    rng = np.random.default_rng(3)
+    reqs = []
+    for k in range(14):
+        r = clmd.Request()
+        r.arrival = 0.002 * k
+        r.natom = int(np.exp(rng.uniform(np.log(150), np.log(7000))))
+        r.rho = float(rng.uniform(0.02, 0.05))
+        r.temp = float(rng.uniform(0.65, 0.75))
+        r.budget = int(rng.choice([300, 450, 800]))
+        r.csover = int(rng.choice([4, 6, 101]))
+        r.seed = 500 + k
+        reqs.append(r)
+    return reqs
+
+
+def test_served_trace_completes_with_pool_admission(gpu):
+    reqs = served_requests()
+    total = sum(r.natom for r in reqs)
+    biggest = max(r.natom for r in reqs)
+    # a pool smaller than the trace: later requests wait for retirements
+    e = clmd.Ensemble(clmd.ens_config(max(biggest, total // 3), 64, ftcsi=50, threads=256))
+    out, st = e.serve(reqs, 300.0)
+    assert st.admitted == len(reqs) and st.completed == len(reqs)
+    assert st.peak_atoms <= max(biggest, total // 3)
+    assert e.free_atoms() == max(biggest, total // 3)  # everything retired
+    for r, o in zip(reqs, out):
+        assert o.done in (1, 2)
+        assert o.admitted >= o.arrival and o.finished >= o.admitted
+        if o.done == 2:
+            assert o.steps == r.budget
+        else:
+            assert o.clbrkt <= o.steps <= r.budget
+    assert any(o.done == 1 for o in out) and any(o.done == 2 for o in out)
+    assert st.atom_steps == sum(o.natom * o.steps for o in out)
+
+
+def test_served_replica_same_alone_and_in_trace(gpu):
+    """Continuous batching changes nothing about a request's trajectory: the
+    served trace and each request served alone agree on steps, outcome and
+    the step the threshold cluster was first seen."""
+    reqs = served_requests()
+    e = clmd.Ensemble(clmd.ens_config(sum(r.natom for r in reqs), 64, ftcsi=50, threads=256))
+    mix, _ = e.serve(reqs, 300.0)
+    for k in (0, 5, 9, 13):
+        a = clmd.Ensemble(clmd.ens_config(reqs[k].natom, 1, ftcsi=50, threads=256))
+        r = clmd.Request()
+        C_ = type(r)
+        for f, _t in C_._fields_:
+            setattr(r, f, getattr(reqs[k], f))
+        r.arrival = 0.0
+        alone, _ = a.serve([r], 300.0)
+        assert (alone[0].steps, alone[0].done, alone[0].clbrkt) == \
+            (mix[k].steps, mix[k].done, mix[k].clbrkt), k
+        a.close()
+
+
+def test_balanced_step_same_trajectories(gpu):
+    """clmd_ens_step_timed only changes how many windows a launch covers:
+    run to the same budget, every replica ends bit-identical to plain steps."""
+    rng = np.random.default_rng(9)
+    specs = [(int(n), float(rng.uniform(0.02, 0.05)), 0.7, 70 + k)
+             for k, n in enumerate([150, 400, 900, 2200, 5000])]
+
+    def build():
+        e = clmd.Ensemble(clmd.ens_config(10000, 8, ftcsi=20, threads=256))
+        slots = []
+        for n, rho, temp, sd in specs:
+            box, arrs = replica_inputs(n, rho, temp, sd)
+            slots.append(e.add(n, box, temp, *arrs, csover=10**6, budget=600))
+        return e, slots
+
+    a, sa = build()
+    while any(r.done == 0 for r in a.results().values()):
+        a.step(1)
+    b, sb = build()
+    launches, small_done = 0, None
+    while any(r.done == 0 for r in b.results().values()):
+        b.step_timed(0.5)
+        launches += 1
+        if small_done is None and b.results()[sb[0]].done:
+            small_done = launches
+    # the largest replica sets the pace (one window per launch); the smallest
+    # ran several windows per launch and finished its 30 windows early
+    assert launches == 30 and small_done < 15
+    for p, q in zip(sa, sb):
+        ra, rb = a.results()[p], b.results()[q]
+        assert (ra.step, ra.done, ra.psi) == (rb.step, rb.done, rb.psi)
+        xa, ca = a.state(p)
+        xb, cb = b.state(q)
+        for k in ("x", "y", "z", "vx", "vy", "vz"):
+            assert np.array_equal(getattr(xa, k), getattr(xb, k)), k
+        assert np.array_equal(ca, cb)
+
+
+def test_nose_hoover_solve_converges_over_long_runs(gpu):
+    """1.5e9 atom-steps of Nose-Hoover without CLMD_ERR_NH_NOCONVERGE.  The
+    reference's per-component relative test (int-verlet-nh-mav.f:140-147)
+    passes because its sweep reaches an exact fixed point; a sweep evaluated
+    with fused multiply-adds does not, and failed here about once per 4e8
+    atom-steps."""
+    rng = np.random.default_rng(12)
+    e = clmd.Ensemble(clmd.ens_config(128 * 4000, 128, ftcsi=100, threads=256))
+    for k in range(128):
+        rho, temp = float(rng.uniform(0.03, 0.05)), float(rng.uniform(0.65, 0.85))
+        box, arrs = replica_inputs(4000, rho, temp, 9000 + k)
+        e.add(4000, box, temp, *arrs, csover=10**6, budget=3000)
+    while any(r.done == 0 and r.status == 0 for r in e.results().values()):
+        e.step(5)
+    res = e.results().values()
+    assert all(r.status == 0 for r in res), [r.status for r in res if r.status]
+    assert all(r.step == 3000 for r in res)
