@@ -112,6 +112,56 @@ __device__ __forceinline__ double cta_max(double v, double* sh) {
   return r;
 }
 
+// two block-wide sums and an "any" flag in one round: every warp reduces the
+// per-warp partials itself, so one barrier publishes them and one guards the
+// buffer's reuse (fixed shape: deterministic)
+template <int NT>
+__device__ __forceinline__ void cta_sum2(double& a, double& b, int& f, double* sh) {
+  constexpr int W = NT / 32;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  a = wsum(a);
+  b = wsum(b);
+  f = __any_sync(0xffffffffu, f);
+  if (lane == 0) {
+    sh[w] = a;
+    sh[W + w] = b;
+    sh[2 * W + w] = f ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  double ta = lane < W ? sh[lane] : 0.0, tb = lane < W ? sh[W + lane] : 0.0;
+  const int tf = lane < W ? (sh[2 * W + lane] != 0.0) : 0;
+  a = wsum(ta);
+  b = wsum(tb);
+  f = __any_sync(0xffffffffu, tf);
+  __syncthreads();
+}
+
+// block max of a and sum of b in one round (as cta_sum2)
+template <int NT>
+__device__ __forceinline__ void cta_maxsum(double& a, double& b, double* sh) {
+  constexpr int W = NT / 32;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  a = wmax(a);
+  b = wsum(b);
+  if (lane == 0) {
+    sh[w] = a;
+    sh[W + w] = b;
+  }
+  __syncthreads();
+  double ta = lane < W ? sh[lane] : 0.0, tb = lane < W ? sh[W + lane] : 0.0;
+  a = wmax(ta);
+  b = wsum(tb);
+  __syncthreads();
+}
+
+// minimum image of a pair difference d in (-L - skin, L + skin): the image
+// the reference's formulas pick for every pair nearer than L/2 (they differ
+// only within rounding of |d| = L/2, beyond every cut-off since the list
+// radius never exceeds L/2), with the same single rounding of d -/+ L
+__device__ __forceinline__ double mi_sel(double d, double L, double hL) {
+  return d > hL ? __dsub_rn(d, L) : (d < -hL ? __dadd_rn(d, L) : d);
+}
+
 __device__ __forceinline__ void kahan(float& s, float& c, float t) {
   float y = __fsub_rn(t, c);
   float u = __fadd_rn(s, y);
@@ -133,7 +183,7 @@ struct Cta {
   double* sz;
   int* cstart;  // [ncell + 1]
   int* cfill;   // [ncell]
-  double red[40];
+  double red[3 * 32 + 8];
   int ncx, ncell, nox, offx[3];
   double cf, rs2;
   int flag;
@@ -335,13 +385,14 @@ __device__ int skin(Rep& R, const Args& A, double dmmr) {
 
 // pair forces (for-a-lj-n-pbc-m.f, sigma = eps = m = 1) -> a; optional
 // velocity-Verlet second half kick; FP64 energy/virial sums when asked
-template <int NT, bool SM, bool MIXED>
+// NHF: also the Nose-Hoover solve's first pass on the fresh accelerations
+// (vo = v: vxn = v, s0 += v.v, dp += b vo dt/Q with b = -dth (a - psi1 vo))
+template <int NT, bool SM, bool MIXED, bool NHF = false>
 __device__ void forces(Rep& R, Cta& C, const Args& A, const Pos<SM>& P, bool kick,
-                       bool energies) {
+                       bool energies, double psi1 = 0.0, double dtQ = 0.0, double* s0 = nullptr,
+                       double* dp = nullptr) {
   const int N = R.natom, off = R.off, tid = threadIdx.x;
-  const double L = R.box, iL = R.ibox, rc2 = A.rc * A.rc, dt = A.dt;
-  const double bf1 = 2.0 + (double)(int)(R.atrskin);
-  const double bf2 = bf1 + 0.5;
+  const double L = R.box, hL = 0.5 * R.box, rc2 = A.rc * A.rc, dt = A.dt;
   const long long lbase = (long long)off * A.lstride;
   double esum = 0.0, vir = 0.0, ek = 0.0;
   for (int i = tid; i < N; i += NT) {
@@ -352,9 +403,9 @@ __device__ void forces(Rep& R, Cta& C, const Args& A, const Pos<SM>& P, bool kic
       float fx = 0.f, fy = 0.f, fz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
       for (int k = 0; k < len; k++) {
         int j = A.list[lbase + (long long)k * N + i];
-        double dx = mi_bf(xi - P.x(j), L, iL, bf1, bf2);
-        double dy = mi_bf(yi - P.y(j), L, iL, bf1, bf2);
-        double dz = mi_bf(zi - P.z(j), L, iL, bf1, bf2);
+        double dx = mi_sel(xi - P.x(j), L, hL);
+        double dy = mi_sel(yi - P.y(j), L, hL);
+        double dz = mi_sel(zi - P.z(j), L, hL);
         double r2d = dx * dx + dy * dy + dz * dz;
         if (r2d <= rc2) {
           float r2 = (float)r2d;
@@ -381,9 +432,9 @@ __device__ void forces(Rep& R, Cta& C, const Args& A, const Pos<SM>& P, bool kic
       double fx = 0.0, fy = 0.0, fz = 0.0;
       for (int k = 0; k < len; k++) {
         int j = A.list[lbase + (long long)k * N + i];
-        double dx = mi_bf(xi - P.x(j), L, iL, bf1, bf2);
-        double dy = mi_bf(yi - P.y(j), L, iL, bf1, bf2);
-        double dz = mi_bf(zi - P.z(j), L, iL, bf1, bf2);
+        double dx = mi_sel(xi - P.x(j), L, hL);
+        double dy = mi_sel(yi - P.y(j), L, hL);
+        double dz = mi_sel(zi - P.z(j), L, hL);
         double r2d = dx * dx + dy * dy + dz * dz;
         if (r2d <= rc2) {
           double ri2 = 1.0 / r2d;
@@ -405,6 +456,19 @@ __device__ void forces(Rep& R, Cta& C, const Args& A, const Pos<SM>& P, bool kic
       ax = fx;
       ay = fy;
       az = fz;
+    }
+    if (NHF) {
+      const double dth = 0.5 * dt;
+      const double V[3] = {A.vx[off + i], A.vy[off + i], A.vz[off + i]};
+      const double a3[3] = {ax, ay, az};
+      A.vxn[off + i] = V[0];
+      A.vyn[off + i] = V[1];
+      A.vzn[off + i] = V[2];
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        *s0 += V[d] * V[d];
+        *dp += (-dth * (a3[d] - psi1 * V[d])) * V[d] * dtQ;
+      }
     }
     if (kick) {
       double vxi = A.vx[off + i] + 0.5 * ax * dt;
@@ -569,6 +633,7 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
   const bool nh = A.integrator == CLMD_INT_NOSE;
   const double dt = A.dt;
   Pos<SM> P{A, C, off};
+  bool vin_n = false;  // uniform: the current velocities are in vxn, not vx
   if (SM) {
     for (int i = tid; i < N; i += NT) {
       C.sx[i] = A.x[off + i];
@@ -626,8 +691,12 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
       // drift
       double d2 = 0.0, sv = 0.0;
       const double psi = R.psi, dt2 = dt * dt / 2, dth = dt / 2;
+      const double* svx = vin_n ? A.vxn : A.vx;
+      const double* svy = vin_n ? A.vyn : A.vy;
+      const double* svz = vin_n ? A.vzn : A.vz;
+      vin_n = false;
       for (int i = tid; i < N; i += NT) {
-        double vxi = A.vx[off + i], vyi = A.vy[off + i], vzi = A.vz[off + i];
+        double vxi = svx[off + i], vyi = svy[off + i], vzi = svz[off + i];
         double axi, ayi, azi;
         get_a<MIXED>(A, off + i, axi, ayi, azi);
         double dx, dy, dz;
@@ -654,8 +723,8 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
         A.vz[off + i] = vzi;
         d2 = fmax(d2, dx * dx + dy * dy + dz * dz);
       }
-      double dmmr = cta_max<NT>(d2, C.red);
-      double sumv2 = nh ? cta_sum<NT>(sv, C.red) : 0.0;
+      cta_maxsum<NT>(d2, sv, C.red);
+      const double dmmr = d2, sumv2 = sv;
       if (tid == 0) {
         if (nh) {
           R.sumv2 = sumv2;
@@ -670,65 +739,56 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
       __syncthreads();
       if (C.flag == 0) goto out;
       if (C.flag == 2 && !rebuild<NT, SM>(R, C, A, P)) goto out;
-      forces<NT, SM, MIXED>(R, C, A, P, !nh, last);
-      if (nh) {
-        // int-verlet-nh-mav.f:91-180 with block reductions
-        const double Q = R.Q, err = 1.0e-10;
-        const double psi1 = R.psi;
-        double s0 = 0.0;
-        for (int i = tid; i < N; i += NT) {
-          double a = A.vx[off + i], b = A.vy[off + i], c = A.vz[off + i];
-          A.vxn[off + i] = a;
-          A.vyn[off + i] = b;
-          A.vzn[off + i] = c;
-          s0 += a * a + b * b + c * c;
-        }
-        double sumv2n = cta_sum<NT>(s0, C.red);
+      if (!nh) {
+        forces<NT, SM, MIXED>(R, C, A, P, true, last);
+      } else {
+        // int-verlet-nh-mav.f:91-180 with block reductions.  Each sweep is one
+        // pass: it updates vn from this sweep's delps and accumulates the
+        // next sweep's sums (sum vn^2, sum b vo dt/Q at pso + delps) in the
+        // same loop; the first pass rides on the force pass.
+        const double Q = R.Q, err = 1.0e-10, psi1 = R.psi, dtQ = dt / Q;
+        double sumv2n = 0.0, dpsum = 0.0;
+        forces<NT, SM, MIXED, true>(R, C, A, P, false, last, psi1, dtQ, &sumv2n, &dpsum);
+        int nr0 = 0;
+        cta_sum2<NT>(sumv2n, dpsum, nr0, C.red);
         double psn = psi1;
         int ready = 0;
         for (int iter = 1; iter <= 1000; iter++) {
-          double pso = psn, dp = 0.0;
-          for (int i = tid; i < N; i += NT) {
-            double ax, ay, az;
-            get_a<MIXED>(A, off + i, ax, ay, az);
-            double vo = A.vxn[off + i];
-            dp += (-dth * (ax - pso * vo) - (A.vx[off + i] - vo)) * vo * dt / Q;
-            vo = A.vyn[off + i];
-            dp += (-dth * (ay - pso * vo) - (A.vy[off + i] - vo)) * vo * dt / Q;
-            vo = A.vzn[off + i];
-            dp += (-dth * (az - pso * vo) - (A.vz[off + i] - vo)) * vo * dt / Q;
-          }
-          double delps = cta_sum<NT>(dp, C.red);
-          double di = -(pso * dth + 1);
-          delps = delps - di * ((-sumv2n + R.nkt3_i) * dth / Q - (psi1 - pso));
+          const double pso = psn;
+          const double di = -(pso * dth + 1);
+          double delps = dpsum - di * ((-sumv2n + R.nkt3_i) * dth / Q - (psi1 - pso));
           delps = delps / (-dt2 * sumv2n / Q + di);
-          double s2 = 0.0;
+          psn = pso + delps;
+          const double rdi = 1.0 / di;
+          double s2 = 0.0, dpn = 0.0;
           int nr = 0;
           for (int i = tid; i < N; i += NT) {
             double ax, ay, az;
             get_a<MIXED>(A, off + i, ax, ay, az);
-            double V[3] = {A.vx[off + i], A.vy[off + i], A.vz[off + i]};
-            double a3[3] = {ax, ay, az};
+            const double V[3] = {A.vx[off + i], A.vy[off + i], A.vz[off + i]};
+            const double a3[3] = {ax, ay, az};
             double* vn[3] = {A.vxn, A.vyn, A.vzn};
-            // int-verlet-nh-mav.f:117-147 rounded term by term: with fused
-            // multiply-adds the residual b never reaches exactly zero, the
-            // sweep keeps moving a near-zero component by ~1e-18 and the
-            // relative test below then fails where the reference converges
+            // the update rounded term by term: with fused multiply-adds the
+            // residual b never reaches exactly zero, the sweep keeps moving a
+            // near-zero component by ~1e-18 and the relative test then fails
+            // where the reference's sweep (int-verlet-nh-mav.f:117-147)
+            // settles on an exact fixed point
 #pragma unroll
             for (int d = 0; d < 3; d++) {
-              double vo = vn[d][off + i];
-              double b = __dsub_rn(__dmul_rn(-dth, __dsub_rn(a3[d], __dmul_rn(pso, vo))),
-                                   __dsub_rn(V[d], vo));
-              double nx =
-                  __dadd_rn(vo, __ddiv_rn(__dadd_rn(b, __dmul_rn(__dmul_rn(dth, vo), delps)), di));
-              if (fabs(__ddiv_rn(__dsub_rn(nx, vo), nx)) > err) nr = 1;
+              const double vo = vn[d][off + i];
+              const double b = __dsub_rn(__dmul_rn(-dth, __dsub_rn(a3[d], __dmul_rn(pso, vo))),
+                                         __dsub_rn(V[d], vo));
+              const double nx =
+                  __dadd_rn(vo, __dmul_rn(__dadd_rn(b, __dmul_rn(__dmul_rn(dth, vo), delps)), rdi));
+              if (fabs(__dsub_rn(nx, vo)) > err * fabs(nx)) nr = 1;
               vn[d][off + i] = nx;
               s2 += nx * nx;
+              dpn += (-dth * (a3[d] - psn * nx) - (V[d] - nx)) * nx * dtQ;
             }
           }
-          sumv2n = cta_sum<NT>(s2, C.red);
-          nr = __syncthreads_or(nr);
-          psn = pso + delps;
+          sumv2n = s2;
+          dpsum = dpn;
+          cta_sum2<NT>(sumv2n, dpsum, nr, C.red);
           if (!nr) {
             ready = 1;
             break;
@@ -739,11 +799,7 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
           __syncthreads();
           goto out;
         }
-        for (int i = tid; i < N; i += NT) {
-          A.vx[off + i] = A.vxn[off + i];
-          A.vy[off + i] = A.vyn[off + i];
-          A.vz[off + i] = A.vzn[off + i];
-        }
+        vin_n = true;  // the step's velocities are in vxn until the next drift
         if (tid == 0) {
           R.sumv2 = sumv2n;
           R.psi = psn;
@@ -751,6 +807,15 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
         }
       }
       if (tid == 0) R.step = step + 1;
+      __syncthreads();
+    }
+    if (vin_n) {  // velocities back in vx for the analysis and the host
+      for (int i = tid; i < N; i += NT) {
+        A.vx[off + i] = A.vxn[off + i];
+        A.vy[off + i] = A.vyn[off + i];
+        A.vz[off + i] = A.vzn[off + i];
+      }
+      vin_n = false;
       __syncthreads();
     }
     // a spent budget ends the replica in this window, after the analysis due
@@ -766,6 +831,13 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
   }
 out:
   __syncthreads();
+  if (vin_n) {
+    for (int i = tid; i < N; i += NT) {
+      A.vx[off + i] = A.vxn[off + i];
+      A.vy[off + i] = A.vyn[off + i];
+      A.vz[off + i] = A.vzn[off + i];
+    }
+  }
   if (SM) {
     for (int i = tid; i < N; i += NT) {
       A.x[off + i] = C.sx[i];
@@ -777,7 +849,7 @@ out:
 }
 
 template <int NT, bool SM, bool MIXED>
-__global__ void __launch_bounds__(NT) k_ens(Args A) {
+__global__ void __launch_bounds__(NT, (NT < 512 ? 512 / NT : 1)) k_ens(Args A) {
   extern __shared__ double dsm[];
   __shared__ Rep R;
   __shared__ Cta C;
