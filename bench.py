@@ -31,6 +31,13 @@ A bench step is one window: every running replica advances 100 steps
 0.7, velocity Verlet, Stillinger every 100 steps), a bench step = one
 analysis cycle of 100 steps.
 
+--workload nvt: one mixed-precision system of N = 2,097,152 atoms (rho* =
+0.05, T* = 0.75, Nose-Hoover with Q = N T* 0.25, FP32 pair terms with Kahan
+FP32 sums, FP64 positions, velocities, PSI and energies), ten Wolde-Frenkel
+clustering (>= 5 neighbours within 1.5 sigma) every 50 steps; a bench step =
+one analysis cycle of 50 steps.  Accelerations stay FP64 in memory (144 B per
+atom-step).
+
 --impl reference times the serial C restatement of the reference (the
 reference is Fortran 77 and no Fortran compiler exists on either machine) on
 the same workload, rank 0 only.
@@ -58,7 +65,13 @@ sys.path.insert(0, PKG)
 import clmd  # noqa: E402
 
 WORKLOAD = dict(name="lj-fp64-dropin", natom=262144, rho=0.02, temp=0.7, rc=2.5, rskin=2.8,
-                atskin=1.5, dt=0.005, nbtim=10, ftcsi=100, seed=1234)
+                atskin=1.5, dt=0.005, nbtim=10, ftcsi=100, seed=1234,
+                integrator=clmd.INT_VERLET, ethst="-", clustering=clmd.CLU_STILLINGER,
+                precision=clmd.PREC_FP64)
+# mixed-precision NVT: Nose-Hoover (Q = N T* 0.25), ten Wolde-Frenkel every 50
+NVT = dict(WORKLOAD, name="lj-mixed-nvt", natom=2097152, rho=0.05, temp=0.75, ftcsi=50,
+           seed=4321, integrator=clmd.INT_NOSE, ethst="N", clustering=clmd.CLU_FRENKEL,
+           precision=clmd.PREC_MIXED)
 BYTES_PER_ATOM_STEP = 144  # FP64: x, v, a read + written
 
 
@@ -68,7 +81,9 @@ def log(*a):
 
 def make_config(w):
     return clmd.lj_config(w["natom"], w["rho"], w["temp"], rc=w["rc"], rskin=w["rskin"],
-                          atskin=w["atskin"], dt=w["dt"], nbtim=w["nbtim"], ftcsi=w["ftcsi"])
+                          atskin=w["atskin"], dt=w["dt"], nbtim=w["nbtim"], ftcsi=w["ftcsi"],
+                          integrator=w["integrator"], ethst=w["ethst"],
+                          clustering=w["clustering"], precision=w["precision"], atnenum=5)
 
 
 def make_state(cfg, seed, temp):
@@ -154,7 +169,7 @@ def cpu_cycle_estimate(w, budget_s=15.0):
         :73-99) timed on a sample of rows at full N, scaled by the pair count,
       - t_label: the Stillinger routine (O(N^2) rescan) timed at N/8 and
         scaled by N^2.
-    Returns (seconds per cycle, description)."""
+    Returns (seconds per cycle of ftcsi steps, description)."""
     sys.path.insert(0, ORACLE)
     import orc
 
@@ -187,8 +202,9 @@ def cpu_cycle_estimate(w, budget_s=15.0):
     t_pairs = time.perf_counter() - t
     t_rebuild = t_pairs / pairs * (n * (n - 1) / 2)
     o.close()
-    # Stillinger labelling at N/8, scaled by N^2
-    ws = dict(w, natom=n // 8)
+    # labelling on a sample of at most 32768 atoms, scaled by N^2
+    div = max(8, n // 32768)
+    ws = dict(w, natom=n // div)
     cfs = make_config(ws)
     sts = make_state(cfs, w["seed"], w["temp"])
     o = orc.Oracle(cfs, neighbor_mode=1)
@@ -196,14 +212,15 @@ def cpu_cycle_estimate(w, budget_s=15.0):
     o.neighbor(0)
     t = time.perf_counter()
     o.stoddard(0)
-    t_label = (time.perf_counter() - t) * 64.0
+    t_label = (time.perf_counter() - t) * float(div * div)
     o.close()
-    rebuilds = 100.0 / w["nbtim"]
-    cycle = 100 * t_step + rebuilds * t_rebuild + t_label
+    cyc = w["ftcsi"]
+    rebuilds = cyc / w["nbtim"]
+    cycle = cyc * t_step + rebuilds * t_rebuild + t_label
     desc = (f"serial oracle, 1 core: {nstep} MD steps at N={n} ({t_step*1e3:.1f} ms/step), "
             f"all-pairs rebuild on {rows} rows ({pairs} pair tests) scaled to N(N-1)/2 "
-            f"({t_rebuild:.1f} s/rebuild, {rebuilds:.0f} per 100 steps), Stillinger labelling "
-            f"at N/8 scaled by 64 ({t_label:.1f} s/analysis)")
+            f"({t_rebuild:.1f} s/rebuild, {rebuilds:.0f} per {cyc} steps), cluster labelling "
+            f"at N/{div} scaled by {div * div} ({t_label:.1f} s/analysis)")
     return cycle, desc
 
 
@@ -221,12 +238,12 @@ def reference_arm(args, w):
         if k >= args.warmup:
             units.append(cyc)
     per_cycle = statistics.mean(units)
-    value = n * 100 / per_cycle
+    value = n * w["ftcsi"] / per_cycle
     line = {
         "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": per_cycle * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "vs_baseline": None, "dtype": w_dtype(w), "data": "synthetic (seeded)",
         "config": config_json(w, args.gpus),
         "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": 1, "kind": "port",
                          "sample": desc},
@@ -236,11 +253,22 @@ def reference_arm(args, w):
     print(json.dumps(line), flush=True)
 
 
+def w_dtype(w):
+    return "f32+f64" if w["precision"] == clmd.PREC_MIXED else "f64"
+
+
 def config_json(w, ngpu):
+    nh = w["integrator"] == clmd.INT_NOSE
     return {"workload": f"{w['name']}-N{w['natom']}-rho{w['rho']}-T{w['temp']}",
             "natom": w["natom"], "rho": w["rho"], "T": w["temp"], "rc": w["rc"],
-            "rskin0": w["rskin"], "dt": w["dt"], "integrator": "velocity-verlet",
-            "clustering": "stillinger-1.5sigma", "steps_per_bench_step": 100,
+            "rskin0": w["rskin"], "dt": w["dt"],
+            "integrator": "nose-hoover (Q = N T* 0.25)" if nh else "velocity-verlet",
+            "precision": "mixed (FP32 pair terms, Kahan FP32 sums)"
+                         if w["precision"] == clmd.PREC_MIXED else "fp64",
+            "clustering": ("ten-wolde-frenkel (>= 5 neighbours within 1.5 sigma)"
+                           if w["clustering"] == clmd.CLU_FRENKEL else "stillinger-1.5sigma")
+                          + f" every {w['ftcsi']}",
+            "steps_per_bench_step": w["ftcsi"],
             "l2": "flushed between timed steps (256 MB write)",
             "parallelism": f"replicas x{ngpu}"}
 
@@ -250,13 +278,18 @@ def config_json(w, ngpu):
 # ---------------------------------------------------------------------------
 def start_system(cfg, state):
     """main.f's start with the writers off: commons from the config
-    (read-3d.f:263-276), stopdead(-1), neighbor(0), a = 0, AccAtom, stoddard(-1)."""
+    (read-3d.f:263-276), stopdead(-1), neighbor(0), a = 0, AccAtom, the
+    Nose-Hoover PSI start (main.f:156-160), stoddard(-1)."""
     g = clmd.System(cfg)
     g.set_state(state, scalars=clmd.scalars_init(cfg))
     g.stopdead(-1)
     g.neighbor(0)
     g.zero_acc()
     g.accatom()
+    if cfg.integrator == clmd.INT_NOSE:
+        s = g.scalars()
+        s.psi = (2.0 * s.ekin - 3.0 * cfg.natom * clmd.CIKB * cfg.att) / cfg.Q
+        g.set_scalars(s)
     g.stoddard(-1)
     return g
 
@@ -354,7 +387,8 @@ def engine_arm(args, w):
     peak, peak_kind = measured_peaks()
     alg = BYTES_PER_ATOM_STEP * n * cyc
     achieved = alg / (kms / 1e3) / 1e9
-    traffic = profiled_traffic()
+    traffic = profiled_traffic("k_cycle_fp64_dropin" if w["name"] == WORKLOAD["name"]
+                               else "k_cycle_mixed_nvt")
 
     # ---- e2e: host buffers through the C ABI
     st_h = g.get_state()
@@ -389,20 +423,22 @@ def engine_arm(args, w):
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             cyc_s, desc = cpu_cycle_estimate(w)
-            cpu = {"value": n * 100 / cyc_s, "unit": "atom-steps/s", "cores": 1, "kind": "port",
+            cpu = {"value": n * cyc / cyc_s, "unit": "atom-steps/s", "cores": 1, "kind": "port",
                    "sample": desc}
         line = {
             "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "vs_baseline": None, "dtype": w_dtype(w), "data": "synthetic (seeded)",
             "config": config_json(w, world),
             "e2e": {"value": e2e_value, "unit": "atom-steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "k_cycle (100 velocity-Verlet steps per launch)",
+                         "kernel": f"k_cycle ({cyc} "
+                                   + ("Nose-Hoover" if w["integrator"] == clmd.INT_NOSE
+                                      else "velocity-Verlet") + " steps per launch)",
                          "algorithmic_bytes_per_launch": alg, "kernel_ms": kms,
                          "peak_kind": peak_kind},
             "cpu_baseline": cpu,
@@ -895,9 +931,10 @@ def main():
     ap.add_argument("--steps", type=int, default=10, help="timed analysis cycles (100 MD steps)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--natom", type=int, default=WORKLOAD["natom"])
+    ap.add_argument("--natom", type=int, default=0, help="dropin/nvt: atoms (0 = the workload's)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="batched", choices=["batched", "dropin", "served"])
+    ap.add_argument("--workload", default="batched",
+                    choices=["batched", "dropin", "nvt", "served"])
     ap.add_argument("--arrival-seconds", type=float, default=1.0,
                     help="served: length of the Poisson arrival window")
     ap.add_argument("--serve-seconds", type=float, default=60.0,
@@ -908,7 +945,10 @@ def main():
     ap.add_argument("--threads", type=int, default=0, help="0 = autotune")
     ap.add_argument("--dropin-sample", type=int, default=8)
     args = ap.parse_args()
-    w = dict(WORKLOAD, natom=args.natom)
+    if args.workload == "nvt":
+        w = dict(NVT, natom=args.natom or NVT["natom"])
+    else:
+        w = dict(WORKLOAD, natom=args.natom or WORKLOAD["natom"])
     if args.workload == "served":
         if args.impl == "reference":
             served_reference_arm(args)

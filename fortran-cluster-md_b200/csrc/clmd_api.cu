@@ -96,6 +96,7 @@ static void fill_params(const clmd_config* c, Params* P) {
   P->clwait = c->clwait;
   P->ftcsi = c->ftcsi;
   P->integrator = c->integrator;
+  P->precision = c->precision == CLMD_PREC_MIXED ? CLMD_PREC_MIXED : CLMD_PREC_FP64;
   P->clustering = c->clustering;
   P->ethst = c->ethst;
   P->clnuctrl = c->clnuctrl;

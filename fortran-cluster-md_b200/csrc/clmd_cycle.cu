@@ -568,6 +568,8 @@ __device__ __forceinline__ void warp_forces(const Params& P, DevState* st, const
   e -= len;  // exclusive prefix: this lane's row starts at wbase + e
   const int wbase = __shfl_sync(FULL, st0, 0);
   const int sa = (int)pa.w;
+  const bool mixed = P.precision == CLMD_PREC_MIXED;
+  float sx = 0.f, sy = 0.f, sz = 0.f, kx = 0.f, ky = 0.f, kz = 0.f;  // mixed: Kahan sums
   fx = 0.0;
   fy = 0.0;
   fz = 0.0;
@@ -605,11 +607,24 @@ __device__ __forceinline__ void warp_forces(const Params& P, DevState* st, const
       double rij2 = dx * dx + dy * dy + dz * dz;
       if (rij2 <= P.atr2) {
         double r2 = rij2;
-        rij2 = 1.0 / rij2;
-        double rij6 = rij2 * rij2 * rij2;
+        double rij6 = 0.0;
+        if (!mixed) {
+          rij2 = 1.0 / rij2;
+          rij6 = rij2 * rij2 * rij2;
+        }
         int ij = osp + (int)pb.w;
         if (ij < 2 || ij > 4) {
           raise_err(st, CLMD_ERR_BAD_SPECIES);
+        } else if (mixed) {
+          double e, w;
+          pair_term_f32(P, ij, r2, dx, dy, dz, tx, ty, tz, e, w);
+          if (own) {
+            esum = esum + e;
+            vir = vir + w;
+            flag = 1;
+          } else {
+            flag = 2;
+          }
         } else {
           double fij = P.eps[ij] * 48.0 * rij2 * rij6 * (P.c2[ij] * rij6 - P.c3[ij]);
           tx = fij * dx;
@@ -635,7 +650,14 @@ __device__ __forceinline__ void warp_forces(const Params& P, DevState* st, const
     for (int a = a0; a < a1; a++) {
       int q = a - c;
       int f = W.flag[q];
-      if (f == 1) {
+      if (mixed) {
+        if (f) {
+          const float sg = f == 1 ? 1.0f : -1.0f;
+          kahan_add(sx, kx, sg * (float)W.tx[q]);
+          kahan_add(sy, ky, sg * (float)W.ty[q]);
+          kahan_add(sz, kz, sg * (float)W.tz[q]);
+        }
+      } else if (f == 1) {
         fx = fx + W.tx[q];
         fy = fy + W.ty[q];
         fz = fz + W.tz[q];
@@ -646,6 +668,11 @@ __device__ __forceinline__ void warp_forces(const Params& P, DevState* st, const
       }
     }
     __syncwarp();
+  }
+  if (mixed) {
+    fx = (double)sx;
+    fy = (double)sy;
+    fz = (double)sz;
   }
 }
 

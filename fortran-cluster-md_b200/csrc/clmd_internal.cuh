@@ -43,6 +43,7 @@ struct Params {
   int ncx_max, ncy_max, ncz_max;
   int list_cap;
   int integrator, clustering;
+  int precision;  // CLMD_PREC_FP64 or CLMD_PREC_MIXED (pair terms)
   char apth[CLMD_MXSORTS];
   char ethst, clnuctrl;
 };
@@ -156,6 +157,34 @@ __device__ __forceinline__ double reduce_partials(const double* p, int n, double
 __device__ __forceinline__ double mimage_bf(double d, double L, double iL, double bf1,
                                             double bf2) {
   return d + L * (bf1 - (double)(int)(bf2 + d * iL));
+}
+
+// Mixed-precision pair term (CLMD_PREC_MIXED): the caller has the FP64
+// minimum-image difference and r^2 (the cut-off test stays FP64); the LJ
+// factors, f_ij and the energy and virial terms are FP32.  t* get the FP32
+// force components (exact in double), e and w the FP32 energy/virial terms.
+__device__ __forceinline__ void pair_term_f32(const Params& P, int ij, double r2d, double dx,
+                                              double dy, double dz, double& tx, double& ty,
+                                              double& tz, double& e, double& w) {
+  const float r2 = (float)r2d;
+  const float ri2 = 1.0f / r2;
+  const float r6 = ri2 * ri2 * ri2;
+  const float eps = (float)P.eps[ij], c1 = (float)P.c1[ij], c2 = (float)P.c2[ij],
+              c3 = (float)P.c3[ij];
+  const float fij = eps * 48.0f * ri2 * r6 * (c2 * r6 - c3);
+  tx = (double)(fij * (float)dx);
+  ty = (double)(fij * (float)dy);
+  tz = (double)(fij * (float)dz);
+  e = (double)(eps * 4.0f * r6 * (c2 * r6 - c1));
+  w = (double)(fij * r2);
+}
+
+// Kahan-compensated FP32 running sum (s += t), rounded step by step
+__device__ __forceinline__ void kahan_add(float& s, float& c, float t) {
+  const float y = __fsub_rn(t, c);
+  const float u = __fadd_rn(s, y);
+  c = __fsub_rn(__fsub_rn(u, s), y);
+  s = u;
 }
 
 // The neighbour-list minimum image (neighbor-pbc-mav.f:84-86).

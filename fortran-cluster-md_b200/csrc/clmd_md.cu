@@ -48,6 +48,8 @@ __global__ void __launch_bounds__(kBlock) k_force(Params P, DevState* st, const 
     double4 pa = pos[i];
     int sa = (int)pa.w;
     double fx = 0.0, fy = 0.0, fz = 0.0;
+    const bool mixed = P.precision == CLMD_PREC_MIXED;
+    float sx = 0.f, sy = 0.f, sz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;  // mixed: Kahan sums
     int k0 = row_start[i], k1 = k0 + row_len[i], kown = k0 + row_lo[i];
     for (int k = k0; k < k1; k++) {
       int j = list[k];
@@ -65,11 +67,27 @@ __global__ void __launch_bounds__(kBlock) k_force(Params P, DevState* st, const 
       double rij2 = dx * dx + dy * dy + dz * dz;
       if (rij2 <= P.atr2) {
         double r2 = rij2;
-        rij2 = 1.0 / rij2;
-        double rij6 = rij2 * rij2 * rij2;
+        double rij6 = 0.0;
+        if (!mixed) {
+          rij2 = 1.0 / rij2;
+          rij6 = rij2 * rij2 * rij2;
+        }
         int ij = sa + (int)pb.w;
         if (ij < 2 || ij > 4) {
           raise_err(st, CLMD_ERR_BAD_SPECIES);
+          continue;
+        }
+        if (mixed) {
+          double tx, ty, tz, e, w;
+          pair_term_f32(P, ij, r2, dx, dy, dz, tx, ty, tz, e, w);
+          const float sg = own ? 1.0f : -1.0f;
+          if (own) {
+            esum = esum + e;
+            vir = vir + w;
+          }
+          kahan_add(sx, cx, sg * (float)tx);
+          kahan_add(sy, cy, sg * (float)ty);
+          kahan_add(sz, cz, sg * (float)tz);
           continue;
         }
         double fij = P.eps[ij] * 48.0 * rij2 * rij6 * (P.c2[ij] * rij6 - P.c3[ij]);
@@ -85,6 +103,11 @@ __global__ void __launch_bounds__(kBlock) k_force(Params P, DevState* st, const 
           fz = fz - fij * dz;
         }
       }
+    }
+    if (mixed) {
+      fx = (double)sx;
+      fy = (double)sy;
+      fz = (double)sz;
     }
     double iatm = 1.0 / P.apmas[sa - 1];
     double a0x = 0.0, a0y = 0.0, a0z = 0.0;

@@ -1,0 +1,118 @@
+"""Mixed precision in the single-system engine (CLMD_PREC_MIXED): FP32 pair
+terms with Kahan-compensated FP32 sums; positions, velocities, the list and
+cluster tests, Nose-Hoover and the energies stay FP64.
+
+Bars: relative force error <= 1e-5 against the FP64 oracle on identical
+positions (normwise, and per atom for atoms above 1% of the largest force);
+list membership bit-exact (the list test is FP64); cluster labels bit-exact
+on identical positions; the Nose-Hoover conserved quantity drifts by the
+same amount as the FP64 engine's within 1e-4 of H per 1e4 steps.
+"""
+import numpy as np
+import pytest
+
+import clmd
+import orc
+from conftest import random_state
+
+pytestmark = pytest.mark.gpu
+
+
+def nvt_config(n, precision, **kw):
+    return clmd.lj_config(n, 0.05, 0.75, integrator=clmd.INT_NOSE, ethst="N",
+                          precision=precision, **kw)
+
+
+def start(cfg, st):
+    """main.f's start: stopdead(-1), neighbor(0), a = 0, AccAtom, PSI
+    (main.f:156-160)."""
+    g = clmd.System(cfg)
+    g.set_state(st, scalars=clmd.scalars_init(cfg))
+    g.stopdead(-1)
+    g.neighbor(0)
+    g.zero_acc()
+    g.accatom()
+    s = g.scalars()
+    s.psi = (2.0 * s.ekin - 3.0 * cfg.natom * clmd.CIKB * cfg.att) / cfg.Q
+    g.set_scalars(s)
+    return g
+
+
+@pytest.mark.parametrize("rho", [0.05, 0.3])
+def test_mixed_forces_against_fp64_oracle(gpu, rho):
+    n = 20000
+    cfg = clmd.lj_config(n, rho, 0.75, precision=clmd.PREC_MIXED)
+    st = random_state(cfg, 31)
+    g = clmd.System(cfg)
+    g.set_state(st, scalars=clmd.scalars_init(cfg))
+    o = orc.Oracle(cfg, neighbor_mode=1)
+    o.set_state(st, scalars=orc.scalars_init(cfg))
+    for s_ in (g, o):
+        s_.neighbor(0)
+        s_.zero_acc()
+        s_.accatom()
+    lg, ig = g.halflist()
+    lo, io = o.halflist()
+    assert np.array_equal(lg, lo) and np.array_equal(ig, io)
+    a, b = g.get_state(), o.get_state()
+    fa = np.stack([a.ax, a.ay, a.az], 1)
+    fb = np.stack([b.ax, b.ay, b.az], 1)
+    assert np.linalg.norm(fa - fb) / np.linalg.norm(fb) <= 1e-5
+    mag = np.linalg.norm(fb, axis=1)
+    big = mag > 0.01 * mag.max()
+    assert (np.linalg.norm(fa - fb, axis=1)[big] / mag[big]).max() <= 1e-5
+    assert abs(g.scalars().epot - o.scalars().epot) <= 1e-6 * abs(o.scalars().epot)
+
+
+def test_mixed_cluster_labels_exact_on_own_positions(gpu):
+    n = 6000
+    cfg = nvt_config(n, clmd.PREC_MIXED, clustering=clmd.CLU_FRENKEL, ftcsi=50)
+    g = start(cfg, random_state(cfg, 8))
+    g.stoddard(-1)
+    g.run(0, 300)
+    st = g.get_state()
+    # both sides from the mixed engine's positions, fresh list radius
+    h = clmd.System(cfg)
+    o = orc.Oracle(cfg, neighbor_mode=1)
+    h.set_state(st, scalars=clmd.scalars_init(cfg))
+    o.set_state(st, scalars=orc.scalars_init(cfg))
+    for s_ in (h, o):
+        s_.neighbor(0)
+        s_.stoddard(7)
+    ch, co = h.clusters(), o.clusters()
+    for k in ("cl", "cs", "csi", "csf", "csif"):
+        assert np.array_equal(ch[k], co[k]), k
+
+
+def nh_energy(g, cfg):
+    q = g.scalars()
+    nkt3 = 3.0 * cfg.natom * clmd.CIKB * cfg.att
+    return q.ekin + q.epot + 0.5 * cfg.Q * q.psi ** 2 + nkt3 * q.s
+
+
+def test_mixed_energy_drift_tracks_fp64(gpu):
+    """H = ekin + epot + Q PSI^2 / 2 + 3 N kT s over 1e4 Nose-Hoover steps.
+    The truncated (unshifted) LJ of the reference loses energy whenever a pair
+    enters the cut-off, so H drifts in FP64 too (about -1.5% per 1e4 steps
+    while the vapour condenses), and how much depends on the trajectory: two
+    FP64 runs whose starts differ by 1e-13 in one velocity end ~2e-4 of H
+    apart.  Mixed precision may add at most 1e-4 of H per 1e4 steps beyond
+    that spread."""
+    n, steps = 200000, 10000
+    st = None
+    drift = {}
+    for name, prec, kick in (("fp64", clmd.PREC_FP64, 0.0), ("fp64'", clmd.PREC_FP64, 1e-13),
+                             ("mixed", clmd.PREC_MIXED, 0.0)):
+        cfg = nvt_config(n, prec, ftcsi=0)
+        if st is None:
+            st = random_state(cfg, 17)
+        s0 = st.copy()
+        s0.vx[0] += kick
+        g = start(cfg, s0)
+        h0 = nh_energy(g, cfg)
+        g.run(0, steps)
+        assert g.scalars().status == 0
+        drift[name] = (nh_energy(g, cfg) - h0) / abs(h0)
+        g.close()
+    spread = abs(drift["fp64'"] - drift["fp64"])
+    assert abs(drift["mixed"] - drift["fp64"]) <= 1e-4 + spread, drift
