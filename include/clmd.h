@@ -267,8 +267,8 @@ int clmd_ens_destroy(clmd_ensemble* e);
 int clmd_ens_add(clmd_ensemble* e, const clmd_replica_spec* spec, const double* x,
                  const double* y, const double* z, const double* vx, const double* vy,
                  const double* vz, int32_t* slot);
-/* Advances every running replica by up to nwin windows (one launch per
- * window, replayed from a CUDA graph); replicas stop when done. */
+/* Advances every running replica by up to nwin windows (one persistent
+ * launch per size class, all windows inside it); replicas stop when done. */
 int clmd_ens_step(clmd_ensemble* e, int32_t nwin);
 /* Balanced step for mixed sizes: every running replica advances by k >= 1
  * windows, k chosen per replica so that each runs for about the same device
