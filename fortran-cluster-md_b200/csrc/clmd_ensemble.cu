@@ -159,7 +159,19 @@ __device__ __forceinline__ void cta_maxsum(double& a, double& b, double* sh) {
 // only within rounding of |d| = L/2, beyond every cut-off since the list
 // radius never exceeds L/2), with the same single rounding of d -/+ L
 __device__ __forceinline__ double mi_sel(double d, double L, double hL) {
-  return d > hL ? __dsub_rn(d, L) : (d < -hL ? __dadd_rn(d, L) : d);
+  if (fabs(d) > hL) d = d > 0.0 ? __dsub_rn(d, L) : __dadd_rn(d, L);
+  return d;
+}
+
+// into [0, L] (neighbor-pbc-mav.f:67-71 up to rounding): between rebuilds an
+// atom moves less than the skin, so one shift suffices; dmod for the rest
+__device__ __forceinline__ double wrap_box(double x, double L) {
+  if (x < 0.0)
+    x = __dadd_rn(x, L);
+  else if (x >= L)
+    x = __dsub_rn(x, L);
+  if (!(x >= 0.0 && x <= L)) x = fmod(fmod(x, L) + L, L);
+  return x;
 }
 
 __device__ __forceinline__ void kahan(float& s, float& c, float t) {
@@ -249,9 +261,7 @@ __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
   for (int c = tid; c < C.ncell; c += NT) C.cfill[c] = 0;
   __syncthreads();
   for (int i = tid; i < N; i += NT) {
-    double x = fmod(fmod(P.x(i), L) + L, L);
-    double y = fmod(fmod(P.y(i), L) + L, L);
-    double z = fmod(fmod(P.z(i), L) + L, L);
+    const double x = wrap_box(P.x(i), L), y = wrap_box(P.y(i), L), z = wrap_box(P.z(i), L);
     P.set(i, x, y, z);
     int cx = min((int)(x * C.cf), C.ncx - 1), cy = min((int)(y * C.cf), C.ncx - 1),
         cz = min((int)(z * C.cf), C.ncx - 1);
@@ -296,25 +306,23 @@ __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
   }
   for (int c = tid; c < C.ncell; c += NT) C.cfill[c] = C.cstart[c];
   __syncthreads();
+  // scatter in arrival order (parent[] is free outside the analysis), then
+  // each atom takes the place of its rank by index inside its cell: the
+  // cell order is fixed whatever the order of the atomics
+  int* tmp = A.parent + off;
   for (int i = tid; i < N; i += NT) {
     int slot = atomicAdd(&C.cfill[A.cellid[off + i]], 1);
-    A.sorted[off + slot] = i;
+    tmp[slot] = i;
   }
   __syncthreads();
-  // order each cell by atom index (fixed row order)
-  for (int c = tid; c < C.ncell; c += NT) {
-    int c0 = C.cstart[c], c1 = C.cstart[c + 1];
-    for (int a = c0 + 1; a < c1; a++) {
-      int key = A.sorted[off + a], b = a - 1;
-      while (b >= c0 && A.sorted[off + b] > key) {
-        A.sorted[off + b + 1] = A.sorted[off + b];
-        b--;
-      }
-      A.sorted[off + b + 1] = key;
-    }
+  for (int i = tid; i < N; i += NT) {
+    const int c = A.cellid[off + i], c0 = C.cstart[c], c1 = C.cstart[c + 1];
+    int r = 0;
+    for (int q = c0; q < c1; q++) r += tmp[q] < i;
+    A.sorted[off + c0 + r] = i;
   }
   __syncthreads();
-  const double iL = R.ibox, rs2 = C.rs2;
+  const double hL = 0.5 * L, rs2 = C.rs2;
   const long long lbase = (long long)off * A.lstride;
   int over = 0;
   for (int i = tid; i < N; i += NT) {
@@ -335,23 +343,32 @@ __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
           xx += xx < 0 ? C.ncx : 0;
           xx -= xx >= C.ncx ? C.ncx : 0;
           int c = (zz * C.ncx + yy) * C.ncx + xx;
-          for (int q = C.cstart[c]; q < C.cstart[c + 1]; q++) {
-            int j = A.sorted[off + q];
-            if (j == i) continue;
-            // the reference's test in its orientation (row of the smaller index)
-            double dx, dy, dz;
-            if (i < j) {
-              dx = xi - P.x(j); dy = yi - P.y(j); dz = zi - P.z(j);
-            } else {
-              dx = P.x(j) - xi; dy = P.y(j) - yi; dz = P.z(j) - zi;
-            }
-            dx = mi_nb(dx, L, iL);
-            dy = mi_nb(dy, L, iL);
-            dz = mi_nb(dz, L, iL);
-            double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-            if (r2 <= rs2) {
-              if (n < A.lstride) A.list[lbase + (long long)n * N + i] = j;
-              n++;
+          const int q1 = C.cstart[c + 1];
+          // four candidates' indices loaded ahead of their tests
+          for (int q = C.cstart[c]; q < q1; q += 4) {
+            int js[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) js[u] = q + u < q1 ? A.sorted[off + q + u] : i;
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+              const int j = js[u];
+              if (j == i) continue;
+              // the pair in the reference's orientation (row of the smaller index)
+              double dx, dy, dz;
+              if (i < j) {
+                dx = xi - P.x(j); dy = yi - P.y(j); dz = zi - P.z(j);
+              } else {
+                dx = P.x(j) - xi; dy = P.y(j) - yi; dz = P.z(j) - zi;
+              }
+              dx = mi_sel(dx, L, hL);
+              dy = mi_sel(dy, L, hL);
+              dz = mi_sel(dz, L, hL);
+              double r2 =
+                  __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+              if (r2 <= rs2) {
+                if (n < A.lstride) A.list[lbase + (long long)n * N + i] = j;
+                n++;
+              }
             }
           }
         }
@@ -409,7 +426,7 @@ __device__ void forces(Rep& R, Cta& C, const Args& A, const Pos<SM>& P, bool kic
         double r2d = dx * dx + dy * dy + dz * dz;
         if (r2d <= rc2) {
           float r2 = (float)r2d;
-          float ri2 = 1.0f / r2;
+          float ri2 = __frcp_rn(r2);
           float r6 = ri2 * ri2 * ri2;
           float fij = 48.0f * ri2 * r6 * (r6 - 0.5f);
           kahan(fx, cx, fij * (float)dx);
