@@ -34,7 +34,7 @@
 namespace clmd_ens {
 
 constexpr int kFptCap = 128;  // first-passage sizes tracked per replica
-constexpr int kNcMax = 20;    // cells per dimension at most (cells never narrower than the list radius)
+constexpr int kNcMax = 28;    // cells per dimension at most (cells never narrower than the list radius)
 
 struct Rep {
   // parameters (reduced units: sigma = eps = m = 1)
@@ -193,8 +193,7 @@ struct Cta {
   double* sx;  // positions in shared memory (nullptr: global)
   double* sy;
   double* sz;
-  int* cstart;  // [ncell + 1]
-  int* cfill;   // [ncell]
+  int* cstart;  // [ncell + 1]: cell c holds sorted[cstart[c] .. cstart[c + 1])
   double red[3 * 32 + 8];
   int ncx, ncell, nox, offx[3];
   double cf, rs2;
@@ -258,7 +257,10 @@ template <int NT, bool SM>
 __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
   const int N = R.natom, off = R.off, tid = threadIdx.x;
   const double L = R.box;
-  for (int c = tid; c < C.ncell; c += NT) C.cfill[c] = 0;
+  // one shared array does the counting sort: counts at cstart[c + 1], an
+  // in-place exclusive scan turns them into starts, and the scatter's
+  // atomics advance each to its cell's end = the next cell's start
+  for (int c = tid; c <= C.ncell; c += NT) C.cstart[c] = 0;
   __syncthreads();
   for (int i = tid; i < N; i += NT) {
     const double x = wrap_box(P.x(i), L), y = wrap_box(P.y(i), L), z = wrap_box(P.z(i), L);
@@ -267,16 +269,17 @@ __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
         cz = min((int)(z * C.cf), C.ncx - 1);
     int c = (cz * C.ncx + cy) * C.ncx + cx;
     A.cellid[off + i] = c;
-    atomicAdd(&C.cfill[c], 1);
+    atomicAdd(&C.cstart[c + 1], 1);
   }
   __syncthreads();
   // exclusive scan of the counts (thread 0 walks warp sums)
   {
     __shared__ int wsums[NT / 32 + 1];
+    int* cnt = C.cstart + 1;
     const int per = (C.ncell + NT - 1) / NT;
     int b0 = tid * per, s = 0;
     for (int k = 0; k < per; k++)
-      if (b0 + k < C.ncell) s += C.cfill[b0 + k];
+      if (b0 + k < C.ncell) s += cnt[b0 + k];
     int lane = tid & 31, w = tid >> 5, incl = s;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -297,21 +300,18 @@ __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
     int ex = wsums[w] + incl - s;
     for (int k = 0; k < per; k++)
       if (b0 + k < C.ncell) {
-        int v = C.cfill[b0 + k];
-        C.cstart[b0 + k] = ex;
+        int v = cnt[b0 + k];
+        cnt[b0 + k] = ex;
         ex += v;
       }
-    if (tid == 0) C.cstart[C.ncell] = N;
     __syncthreads();
   }
-  for (int c = tid; c < C.ncell; c += NT) C.cfill[c] = C.cstart[c];
-  __syncthreads();
   // scatter in arrival order (parent[] is free outside the analysis), then
   // each atom takes the place of its rank by index inside its cell: the
   // cell order is fixed whatever the order of the atomics
   int* tmp = A.parent + off;
   for (int i = tid; i < N; i += NT) {
-    int slot = atomicAdd(&C.cfill[A.cellid[off + i]], 1);
+    int slot = atomicAdd(&C.cstart[A.cellid[off + i] + 1], 1);
     tmp[slot] = i;
   }
   __syncthreads();
@@ -338,14 +338,23 @@ __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
         int yy = cy + C.offx[b];
         yy += yy < 0 ? C.ncx : 0;
         yy -= yy >= C.ncx ? C.ncx : 0;
-        for (int d = 0; d < C.nox; d++) {
-          int xx = cx + C.offx[d];
-          xx += xx < 0 ? C.ncx : 0;
-          xx -= xx >= C.ncx ? C.ncx : 0;
-          int c = (zz * C.ncx + yy) * C.ncx + xx;
-          const int q1 = C.cstart[c + 1];
+        // the x-neighbours of a cell row are contiguous in cell order: one
+        // candidate range, two where the row wraps (all of it when ncx <= 2)
+        const int rowc = (zz * C.ncx + yy) * C.ncx;
+        int ra[2], rb[2], nr = 1;
+        if (C.nox < 3) {
+          ra[0] = rowc; rb[0] = rowc + C.ncx;
+        } else if (cx == 0) {
+          ra[0] = rowc; rb[0] = rowc + 2; ra[1] = rowc + C.ncx - 1; rb[1] = rowc + C.ncx; nr = 2;
+        } else if (cx == C.ncx - 1) {
+          ra[0] = rowc + cx - 1; rb[0] = rowc + C.ncx; ra[1] = rowc; rb[1] = rowc + 1; nr = 2;
+        } else {
+          ra[0] = rowc + cx - 1; rb[0] = rowc + cx + 2;
+        }
+        for (int d = 0; d < nr; d++) {
+          const int q1 = C.cstart[rb[d]];
           // four candidates' indices loaded ahead of their tests
-          for (int q = C.cstart[c]; q < q1; q += 4) {
+          for (int q = C.cstart[ra[d]]; q < q1; q += 4) {
             int js[4];
 #pragma unroll
             for (int u = 0; u < 4; u++) js[u] = q + u < q1 ? A.sorted[off + q + u] : i;
@@ -889,8 +898,7 @@ __global__ void __launch_bounds__(NT, (NT < 512 ? 512 / NT : 1)) k_ens(Args A) {
       const int ncell = R.ncmax * R.ncmax * R.ncmax;
       C.rep = r;
       C.cstart = (int*)dsm;
-      C.cfill = C.cstart + (ncell + 1);
-      double* p = (double*)(C.cfill + ncell + 1);
+      double* p = (double*)(C.cstart + ((ncell + 2) & ~1));
       C.sx = SM ? p : nullptr;
       C.sy = SM ? p + nmax : nullptr;
       C.sz = SM ? p + 2 * nmax : nullptr;
@@ -975,7 +983,7 @@ static int ck(cudaError_t e, const char* w) {
 
 static size_t smem_bytes(int nmax, int ncmax, bool sm) {
   size_t nc = (size_t)ncmax * ncmax * ncmax;
-  return sizeof(int) * (2 * nc + 2) + (sm ? 3 * sizeof(double) * (size_t)nmax : 0);
+  return sizeof(int) * ((nc + 2) & ~(size_t)1) + (sm ? 3 * sizeof(double) * (size_t)nmax : 0);
 }
 
 // the largest cell grid that fits beside the resident positions (at least
@@ -1189,7 +1197,9 @@ extern "C" int clmd_ens_add(clmd_ensemble* E, const clmd_replica_spec* sp, const
   R.dmmsu = 256.0 * (E->cfg.rskin - E->cfg.rc) / (double)(float)E->cfg.nbtim;
   R.cstep = -1;
   bool fits = false;
-  R.ncmax = cells_for(E->smem_cap, N, &fits);
+  // the cell grid never needs more than box / rc cells per dimension (the
+  // list radius stays above rc): small boxes keep their shared memory small
+  R.ncmax = std::max(1, std::min(cells_for(E->smem_cap, N, &fits), (int)(sp->box / E->cfg.rc)));
   ECK(cudaMemcpyAsync(A.reps + s, &R, sizeof(Rep), cudaMemcpyHostToDevice, st));
   E->h_summary[s] = make_int4(0, 0, 0, 0);
   ECK(cudaMemcpyAsync(A.summary + s, &E->h_summary[s], sizeof(int4), cudaMemcpyHostToDevice,
