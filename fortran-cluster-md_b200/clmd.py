@@ -589,10 +589,10 @@ class Ensemble:
         if st:
             raise ClmdError(st, "clmd_ens_step")
 
-    def step_timed(self, min_ms):
-        """Balanced step: each replica runs as many windows as fit in about
-        max(min_ms, the longest one-window time) of device time."""
-        st = self.lib.clmd_ens_step_timed(self.h, min_ms)
+    def step_timed(self, ms):
+        """Balanced step: each replica runs as many MD steps as fit in about
+        ms of device time (at least one)."""
+        st = self.lib.clmd_ens_step_timed(self.h, ms)
         if st:
             raise ClmdError(st, "clmd_ens_step_timed")
 

@@ -57,7 +57,7 @@ struct Args {
   int *list, *rlen, *sorted, *cellid, *parent, *cs, *cl, *fpt;
   Rep* reps;
   const int* items;
-  const int* iwin;  // windows per item (nullptr: nwin for every item)
+  const int* iwin;  // MD steps per item (nullptr: nwin windows for every item)
   int nitems;
   int* ctr;
   double rc, atskin, dt;
@@ -199,7 +199,7 @@ struct Cta {
   double cf, rs2;
   int flag;
   int rep;  // slot of the replica being run
-  int nwin;  // windows this replica runs in this launch
+  int nsteps;  // MD steps this replica runs in this launch
 };
 
 template <bool SM>
@@ -698,21 +698,33 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
     }
     __syncthreads();
   }
-  for (int w = 0; w < C.nwin; w++) {
+  // C.nsteps MD steps in this launch; the analysis and chk_nucleation run
+  // whenever the step counter reaches a multiple of ftcsi (wrt-csi.f:27,
+  // main.f:157-161), wherever the launch boundaries fall
+  for (int todo = C.nsteps; todo > 0; todo--) {
     if (R.done || R.status) break;
-    // wrt-csi.f:27 + chk_nucleation (main.f:157-161) at an analysis step
     if (A.ftcsi > 0 && R.step % A.ftcsi == 0 && R.cstep != R.step) {
+      if (vin_n) {  // velocities back in vx for the analysis
+        for (int i = tid; i < N; i += NT) {
+          A.vx[off + i] = A.vxn[off + i];
+          A.vy[off + i] = A.vyn[off + i];
+          A.vz[off + i] = A.vzn[off + i];
+        }
+        vin_n = false;
+        __syncthreads();
+      }
       analysis<NT, SM>(R, C, A, P, R.step);
       if (R.done) break;
     }
-    const int nsteps = A.ftcsi > 0 ? A.ftcsi : 1;
-    for (int s = 0; s < nsteps; s++) {
-      if (R.step >= R.budget) {
-        if (tid == 0) R.done = 2;
-        __syncthreads();
-        break;
-      }
-      const bool last = (s == nsteps - 1);
+    if (R.step >= R.budget) {
+      __syncthreads();
+      if (tid == 0) R.done = 2;
+      __syncthreads();
+      break;
+    }
+    {
+      // energies at the end of every window and of the launch
+      const bool last = todo == 1 || (R.step + 1) % (A.ftcsi > 0 ? A.ftcsi : 1) == 0;
       const int step = R.step;
       // drift
       double d2 = 0.0, sv = 0.0;
@@ -835,24 +847,24 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
       if (tid == 0) R.step = step + 1;
       __syncthreads();
     }
-    if (vin_n) {  // velocities back in vx for the analysis and the host
-      for (int i = tid; i < N; i += NT) {
-        A.vx[off + i] = A.vxn[off + i];
-        A.vy[off + i] = A.vyn[off + i];
-        A.vz[off + i] = A.vzn[off + i];
+    // a spent budget ends the replica at once, after the analysis due at its
+    // last step, rather than at the start of the next launch
+    if (R.step >= R.budget) {
+      if (vin_n) {
+        for (int i = tid; i < N; i += NT) {
+          A.vx[off + i] = A.vxn[off + i];
+          A.vy[off + i] = A.vyn[off + i];
+          A.vz[off + i] = A.vzn[off + i];
+        }
+        vin_n = false;
+        __syncthreads();
       }
-      vin_n = false;
-      __syncthreads();
-    }
-    // a spent budget ends the replica in this window, after the analysis due
-    // at its last step, rather than at the start of the next window
-    const bool spent = R.step >= R.budget && !R.done && !R.status;
-    __syncthreads();
-    if (spent) {
       if (A.ftcsi > 0 && R.step % A.ftcsi == 0 && R.cstep != R.step)
         analysis<NT, SM>(R, C, A, P, R.step);
+      __syncthreads();
       if (tid == 0 && !R.done) R.done = 2;
       __syncthreads();
+      break;
     }
   }
 out:
@@ -907,7 +919,7 @@ __global__ void __launch_bounds__(NT, (NT < 512 ? 512 / NT : 1)) k_ens(Args A) {
     unsigned long long t0 = 0;
     const int step0 = R.step;
     if (threadIdx.x == 0) {
-      C.nwin = A.iwin ? A.iwin[it] : A.nwin;
+      C.nsteps = A.iwin ? A.iwin[it] : A.nwin * (A.ftcsi > 0 ? A.ftcsi : 1);
       asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
     }
     __syncthreads();
@@ -1291,10 +1303,10 @@ static int launch_class(clmd_ensemble* E, int c, int item0, int nitems, const in
 
 // all running replicas, split by size class, each class largest first; the
 // classes run concurrently on their own streams
-// min_ms > 0: balanced launch -- replica i runs nwin * k_i windows, k_i =
-// max(1, floor(T / t_i)), t_i its measured one-window device time and T =
-// max(min_ms, max t_i), so that every CTA stays busy about as long as the
-// longest replica's window (a replica not yet timed runs nwin windows)
+// min_ms > 0: balanced launch -- replica i runs max(1, floor(min_ms / t_i))
+// steps, t_i its device time per step measured in its earlier launches, so
+// that every CTA stays busy about min_ms whatever its replica's size (a
+// replica not yet timed runs a few steps)
 static int launch_all(clmd_ensemble* E, int nwin, const int* threads, float min_ms = 0.0f) {
   std::vector<int> cls[clmd_ensemble::kClasses];
   int nmax[clmd_ensemble::kClasses] = {};
@@ -1317,14 +1329,11 @@ static int launch_all(clmd_ensemble* E, int nwin, const int* threads, float min_
   }
   const bool balanced = min_ms > 0.0f;
   if (balanced && total > 0) {
-    const int wsteps = E->cfg.ftcsi > 0 ? E->cfg.ftcsi : 1;
-    float T = min_ms;
-    for (int k = 0; k < total; k++) T = std::max(T, E->h_wtime[E->h_items[k]] * wsteps);
-    for (int k = 0; k < total; k++) {
-      const float t = E->h_wtime[E->h_items[k]] * wsteps;
-      long long w = t > 0.0f ? (long long)(T / t) : 1;
-      w = std::max(1LL, std::min(w, 4096LL)) * nwin;
-      E->h_iwin[k] = (int)std::min(w, (long long)1 << 24);
+    const int win = E->cfg.ftcsi > 0 ? E->cfg.ftcsi : 1;
+    for (int k = 0; k < total; k++) {  // a replica not timed yet runs a few steps
+      const float t = E->h_wtime[E->h_items[k]];  // ms per step, 0 = not timed yet
+      long long n = t > 0.0f ? (long long)(min_ms / t) : (long long)std::min(win, 10);
+      E->h_iwin[k] = (int)std::max(1LL, std::min(n, (long long)1 << 24));
     }
     ECK(cudaMemcpyAsync(E->d_iwin, E->h_iwin, sizeof(int) * total, cudaMemcpyHostToDevice,
                         E->stream));
@@ -1526,10 +1535,18 @@ extern "C" int clmd_ens_fpt(clmd_ensemble* E, int32_t slot, int32_t* fpt, int32_
 }
 
 // slot-ordered host ranges of every occupied slot
-static void host_ranges(clmd_ensemble* E, std::vector<std::pair<long long, int>>& r) {
+// pool ranges of the occupied slots in slot order (the host layout), with
+// consecutive slots whose pool ranges abut merged into one copy
+static void host_ranges(clmd_ensemble* E, std::vector<std::pair<long long, long long>>& r) {
   r.clear();
-  for (int s = 0; s < E->cfg.max_replicas; s++)
-    if (E->used[s]) r.push_back({E->slot_off[s], E->h_reps[s].natom});
+  for (int s = 0; s < E->cfg.max_replicas; s++) {
+    if (!E->used[s]) continue;
+    const long long off = E->slot_off[s], n = E->h_reps[s].natom;
+    if (!r.empty() && r.back().first + r.back().second == off)
+      r.back().second += n;
+    else
+      r.push_back({off, n});
+  }
 }
 
 extern "C" int clmd_ens_upload(clmd_ensemble* E, const double* x, const double* y,
@@ -1537,7 +1554,7 @@ extern "C" int clmd_ens_upload(clmd_ensemble* E, const double* x, const double* 
                                const double* vz) {
   if (!E) return CLMD_ERR_ARG;
   std::lock_guard<std::mutex> lock(E->mu);
-  std::vector<std::pair<long long, int>> r;
+  std::vector<std::pair<long long, long long>> r;
   host_ranges(E, r);
   const double* src[6] = {x, y, z, vx, vy, vz};
   double* dst[6] = {E->A.x, E->A.y, E->A.z, E->A.vx, E->A.vy, E->A.vz};
@@ -1558,7 +1575,7 @@ extern "C" int clmd_ens_download(clmd_ensemble* E, double* x, double* y, double*
                                  double* vx, double* vy, double* vz) {
   if (!E) return CLMD_ERR_ARG;
   std::lock_guard<std::mutex> lock(E->mu);
-  std::vector<std::pair<long long, int>> r;
+  std::vector<std::pair<long long, long long>> r;
   host_ranges(E, r);
   double* dst[6] = {x, y, z, vx, vy, vz};
   const double* src[6] = {E->A.x, E->A.y, E->A.z, E->A.vx, E->A.vy, E->A.vz};

@@ -77,9 +77,10 @@ class Generator {
   std::mutex mu_;
 };
 
-// device time of one round at least: rounds shorter than this spend a
-// noticeable share on launches and the per-round host work
-constexpr float kMinRoundMs = 10.0f;
+// device time of one round: every resident replica advances about this long
+// between two admission points; much shorter rounds spend a noticeable share
+// on launches and the per-round host work
+constexpr float kMinRoundMs = 25.0f;
 
 double now_s(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

@@ -267,17 +267,17 @@ int clmd_ens_destroy(clmd_ensemble* e);
 int clmd_ens_add(clmd_ensemble* e, const clmd_replica_spec* spec, const double* x,
                  const double* y, const double* z, const double* vx, const double* vy,
                  const double* vz, int32_t* slot);
-/* Advances every running replica by up to nwin windows (one persistent
- * launch per size class, all windows inside it); replicas stop when done. */
+/* Advances every running replica by up to nwin windows of ftcsi steps (one
+ * persistent launch per size class); replicas stop when done. */
 int clmd_ens_step(clmd_ensemble* e, int32_t nwin);
-/* Balanced step for mixed sizes: every running replica advances by k >= 1
- * windows, k chosen per replica so that each runs for about the same device
- * time T = max(min_ms, the longest one-window time among them), from window
- * times the kernel measured per replica in earlier launches (a replica not
- * yet timed runs one window).  Small replicas then do not idle while the
- * largest finishes its window.  Trajectories are those of clmd_ens_step:
- * only how many windows one launch covers differs. */
-int clmd_ens_step_timed(clmd_ensemble* e, float min_ms);
+/* Balanced step for mixed sizes: every running replica advances for about
+ * ms of device time (at least one MD step), from the time per step the
+ * kernel measured for it in earlier launches (a replica not yet timed runs
+ * a few steps).  Small replicas then do not idle while the largest finish,
+ * and a launch lasts about ms whatever the sizes.  Launch boundaries may
+ * fall inside a window: the analysis still runs at every multiple of ftcsi,
+ * and trajectories are those of clmd_ens_step. */
+int clmd_ens_step_timed(clmd_ensemble* e, float ms);
 /* Autotuner: picks the block size of each of the 4 replica-size classes
  * (atoms <= 1024, <= 2560, <= 6144, larger) from {128, 256, 512, 1024} by
  * timing one window per candidate on the running replicas; those 4 windows
