@@ -284,6 +284,14 @@ def load(path: str = LIB_PATH):
                         C.POINTER(RequestResult), C.POINTER(ServeStats)], C.c_int),
         "clmd_ens_get_state": ([P, C.c_int32, d, d, d, d, d, d, d, d, d, i], C.c_int),
         "clmd_ens_fpt": ([P, C.c_int32, i, C.c_int32], C.c_int),
+        "clmd_ens_mfpt": ([P, C.c_int32, d, d, i], C.c_int),
+        "clmd_get_config": ([P, C.POINTER(Config)], C.c_int),
+        "clmd_write_rst": ([P, C.c_char_p, C.c_int32], C.c_int),
+        "clmd_read_rst": ([P, C.c_char_p, i], C.c_int),
+        "clmd_write_csi": ([P, C.c_int32, C.c_char_p, C.c_char_p], C.c_int),
+        "clmd_write_fpt": ([P, C.c_char_p], C.c_int),
+        "clmd_ens_write_rst": ([P, C.c_int32, C.c_char_p, C.c_int32], C.c_int),
+        "clmd_ens_write_fpt": ([P, C.c_int32, C.c_double, C.c_char_p], C.c_int),
         "clmd_ens_upload": ([P, d, d, d, d, d, d], C.c_int),
         "clmd_ens_last_ms": ([P, C.POINTER(C.c_float), C.POINTER(C.c_int64)], C.c_int),
         "clmd_ens_download": ([P, d, d, d, d, d, d], C.c_int),
@@ -511,6 +519,27 @@ class System:
         return self.lib.clmd_kernel_launches(self.h)
 
     # -- outputs -------------------------------------------------------------
+    def write_rst(self, path, mxa=0):
+        """wrt-rst.f: the reference's restart file (+ the engine record)."""
+        self._chk(self.lib.clmd_write_rst(self.h, os.fsencode(path), mxa), "write_rst")
+
+    def read_rst(self, path):
+        """read-rst.f: state from a restart file, then neighbor(btim);
+        returns btim."""
+        st = C.c_int32(0)
+        self._chk(self.lib.clmd_read_rst(self.h, os.fsencode(path), C.byref(st)), "read_rst")
+        return st.value
+
+    def write_csi(self, step, csi_path, fsi_path=None):
+        """wrt-csi.f / wrt-csi-fre.f: append this analysis to the files."""
+        self._chk(self.lib.clmd_write_csi(self.h, step, os.fsencode(csi_path),
+                                          os.fsencode(fsi_path) if fsi_path else None),
+                  "write_csi")
+
+    def write_fpt(self, path):
+        """wrt-fpt.f: append the first-passage table."""
+        self._chk(self.lib.clmd_write_fpt(self.h, os.fsencode(path)), "write_fpt")
+
     def halflist(self):
         """(atnlist, atnidx) in the reference's layout (1-based values)."""
         n = C.c_int64(0)
@@ -657,6 +686,27 @@ class Ensemble:
         if st:
             raise ClmdError(st, "clmd_ens_fpt")
         return a
+
+    def mfpt(self, cap=128):
+        """Per size 1..cap: (mean first-passage step, standard error, count)
+        over the occupied slots (helpers/mpt.f on the device)."""
+        mean, sem = np.zeros(cap), np.zeros(cap)
+        cnt = np.zeros(cap, dtype=np.int32)
+        st = self.lib.clmd_ens_mfpt(self.h, cap, ptr(mean, C.c_double), ptr(sem, C.c_double),
+                                    ptr(cnt, C.c_int32))
+        if st:
+            raise ClmdError(st, "clmd_ens_mfpt")
+        return mean, sem, cnt
+
+    def write_rst(self, slot, path, mxa=0):
+        st = self.lib.clmd_ens_write_rst(self.h, slot, os.fsencode(path), mxa)
+        if st:
+            raise ClmdError(st, "clmd_ens_write_rst")
+
+    def write_fpt(self, slot, dt, path):
+        st = self.lib.clmd_ens_write_fpt(self.h, slot, dt, os.fsencode(path))
+        if st:
+            raise ClmdError(st, "clmd_ens_write_fpt")
 
     def last_ms(self):
         """Device ms and atoms of the last window, per size class."""

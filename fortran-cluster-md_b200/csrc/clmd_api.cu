@@ -343,6 +343,12 @@ extern "C" int clmd_get_scalars(clmd_system* S, clmd_scalars* sc) {
   return set_last(CLMD_OK);
 }
 
+extern "C" int clmd_get_config(clmd_system* S, clmd_config* cfg) {
+  if (!S || !cfg) return set_last(CLMD_ERR_ARG);
+  *cfg = S->cfg;
+  return set_last(CLMD_OK);
+}
+
 extern "C" int clmd_set_scalars(clmd_system* S, const clmd_scalars* sc) {
   return clmd_set_state(S, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
                         nullptr, nullptr, nullptr, sc);

@@ -1534,7 +1534,68 @@ extern "C" int clmd_ens_fpt(clmd_ensemble* E, int32_t slot, int32_t* fpt, int32_
   return CLMD_OK;
 }
 
-// slot-ordered host ranges of every occupied slot
+// helpers/mpt.f:80-92 over the replicas instead of over sizer files: per
+// size, the mean first-passage step of the replicas whose largest cluster
+// reached it, and its standard error sqrt((<t^2> - <t>^2) / count); sums in
+// slot order (deterministic)
+__global__ void k_mfpt(const int* fpt, const int* use, int nslot, int cap, double* mean,
+                       double* sem, int* count) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= cap) return;
+  double t = 0.0, tt = 0.0;
+  int n = 0;
+  for (int s = 0; s < nslot; s++) {
+    if (!use[s]) continue;
+    const int v = fpt[(size_t)s * kFptCap + j];
+    if (v < 0) continue;
+    const double d = (double)v;
+    t += d;
+    tt += d * d;
+    n++;
+  }
+  count[j] = n;
+  if (n == 0) {
+    mean[j] = -1.0;
+    sem[j] = 0.0;
+    return;
+  }
+  const double m = t / (double)n;
+  mean[j] = m;
+  sem[j] = sqrt(fmax(tt / (double)n - m * m, 0.0) / (double)n);
+}
+
+extern "C" int clmd_ens_mfpt(clmd_ensemble* E, int32_t cap, double* mean, double* sem,
+                             int32_t* count) {
+  if (!E || !mean || !sem || !count || cap < 1) return CLMD_ERR_ARG;
+  std::lock_guard<std::mutex> lock(E->mu);
+  const int n = std::min(cap, kFptCap), R = E->cfg.max_replicas;
+  int* d_use = nullptr;
+  double* d_out = nullptr;
+  int* d_cnt = nullptr;
+  ECK(cudaMalloc(&d_use, sizeof(int) * R));
+  ECK(cudaMalloc(&d_out, sizeof(double) * 2 * n));
+  ECK(cudaMalloc(&d_cnt, sizeof(int) * n));
+  std::vector<int> use(E->used.begin(), E->used.end());
+  cudaStream_t st = E->stream;
+  ECK(cudaMemcpyAsync(d_use, use.data(), sizeof(int) * R, cudaMemcpyHostToDevice, st));
+  k_mfpt<<<(n + 127) / 128, 128, 0, st>>>(E->A.fpt, d_use, R, n, d_out, d_out + n, d_cnt);
+  E->launches++;
+  ECK(cudaGetLastError());
+  ECK(cudaMemcpyAsync(mean, d_out, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  ECK(cudaMemcpyAsync(sem, d_out + n, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  ECK(cudaMemcpyAsync(count, d_cnt, sizeof(int) * n, cudaMemcpyDeviceToHost, st));
+  ECK(cudaStreamSynchronize(st));
+  cudaFree(d_use);
+  cudaFree(d_out);
+  cudaFree(d_cnt);
+  for (int k = n; k < cap; k++) {
+    mean[k] = -1.0;
+    sem[k] = 0.0;
+    count[k] = 0;
+  }
+  return CLMD_OK;
+}
+
 // pool ranges of the occupied slots in slot order (the host layout), with
 // consecutive slots whose pool ranges abut merged into one copy
 static void host_ranges(clmd_ensemble* E, std::vector<std::pair<long long, long long>>& r) {

@@ -157,6 +157,8 @@ int clmd_get_state(clmd_system* sys, double* x, double* y, double* z,
                    double* vx, double* vy, double* vz,
                    double* ax, double* ay, double* az, clmd_scalars* sc);
 int clmd_get_scalars(clmd_system* sys, clmd_scalars* sc);
+/* The configuration the system was created with. */
+int clmd_get_config(clmd_system* sys, clmd_config* cfg);
 int clmd_set_scalars(clmd_system* sys, const clmd_scalars* sc);
 int clmd_clear_status(clmd_system* sys);
 
@@ -308,6 +310,42 @@ int clmd_ens_download(clmd_ensemble* e, double* x, double* y, double* z, double*
 /* First step at which the largest cluster reached each size 1..cap (-1 if
  * not yet). */
 int clmd_ens_fpt(clmd_ensemble* e, int32_t slot, int32_t* fpt, int32_t cap);
+/* ---- restart files and analysis writers ---------------------------------
+ * wrt-rst.f:30-45: the reference's restart file, a gfortran unformatted
+ * sequential file (each record framed by its 4-byte length): mxa;
+ * (ekin, epot, ekin, epot, ekin); (ewall, ewallsum, fwall, fwallsum), zero
+ * here (no wall); x0,y0,z0; x1,y1,z1; x2,y2,z2; and the Gear derivatives
+ * x3..z5, zero here; every array padded to mxa entries (mxa <= 0: natom).
+ * One more record follows the reference's ones: the engine state that the
+ * reference would rebuild from the deck (PSI, s, the adaptive list radius,
+ * the displacement ring, the cluster cursors), tagged "CLMDSC01" + the
+ * clmd_scalars struct.  A Fortran readRST never reads past its own records. */
+int clmd_write_rst(clmd_system* sys, const char* path, int32_t mxa);
+/* read-rst.f:37-65: loads x, v, a and (ekin, epot) from such a file (its mxa
+ * must hold natom atoms, else CLMD_ERR_ARG), the engine record when present,
+ * then rebuilds the list as the reference does: step = btim,
+ * neighbor(step).  *step (may be NULL) gets btim. */
+int clmd_read_rst(clmd_system* sys, const char* path, int32_t* step);
+/* wrt-csi.f (Stillinger) / wrt-csi-fre.f:32-57 (ten Wolde-Frenkel): appends
+ * this step's cluster-size distribution from the last stoddard() to
+ * csi_path and, for ten Wolde-Frenkel, the liquid-cluster one to fsi_path
+ * (NULL: skipped), in the reference's fixed formats. */
+int clmd_write_csi(clmd_system* sys, int32_t step, const char* csi_path, const char* fsi_path);
+/* wrt-fpt.f:30-37: the first-passage table (size, Stillinger time, tWF time
+ * in the reference's dt*1e6 units), appended to path. */
+int clmd_write_fpt(clmd_system* sys, const char* path);
+/* One replica's restart file (reference records; its engine record, tagged
+ * "CLMDRP01", is the replica's clmd_replica_result) and its first-passage table in the
+ * wrt-fpt.f layout (Stillinger column; the tWF column is -1 / the
+ * reference's placeholder). */
+int clmd_ens_write_rst(clmd_ensemble* e, int32_t slot, const char* path, int32_t mxa);
+int clmd_ens_write_fpt(clmd_ensemble* e, int32_t slot, double dt, const char* path);
+/* Mean first-passage statistics over the occupied slots, on the device
+ * (helpers/passage-time.f + helpers/mpt.f:80-92 in one pass): for each size
+ * j = 1..cap, count[j-1] replicas whose largest cluster reached j, the mean
+ * of their first-passage steps (-1 when none) and its standard error
+ * sqrt((<t^2> - <t>^2) / count).  Steps, not time: multiply by dt. */
+int clmd_ens_mfpt(clmd_ensemble* e, int32_t cap, double* mean, double* sem, int32_t* count);
 /* Device time (ms, CUDA events) of the last window's launch of each of the 4
  * size classes (-1 if the class was empty) and the atoms it advanced. */
 int clmd_ens_last_ms(clmd_ensemble* e, float* ms, int64_t* atoms);

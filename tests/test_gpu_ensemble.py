@@ -277,3 +277,33 @@ def test_bulk_upload_download_in_slot_order(gpu):
         assert np.array_equal(bufs[0][h:h + n], st.x)
         assert np.array_equal(bufs[5][h:h + n], st.vz)
         h += n
+
+
+def test_mean_first_passage_matches_per_replica_tables(gpu):
+    """clmd_ens_mfpt (helpers/passage-time.f + mpt.f on the device) against
+    the same statistics computed here from every replica's first-passage
+    table (clmd_ens_fpt)."""
+    rng = np.random.default_rng(21)
+    e = clmd.Ensemble(clmd.ens_config(60 * 1500, 64, ftcsi=25, threads=256))
+    slots = []
+    for k in range(60):
+        n = int(rng.integers(300, 1500))
+        box, arrs = replica_inputs(n, float(rng.uniform(0.03, 0.05)), 0.65, 700 + k)
+        slots.append(e.add(n, box, 0.65, *arrs, csover=10**6, budget=400))
+    e.remove(slots[7])  # a freed slot does not count
+    del slots[7]
+    e.step(20)
+    cap = 64
+    mean, sem, cnt = e.mfpt(cap)
+    tab = np.array([e.fpt(s, cap) for s in sorted(slots)], dtype=np.int64)
+    for j in range(cap):
+        t = tab[:, j][tab[:, j] >= 0].astype(np.float64)
+        assert cnt[j] == len(t)
+        if len(t) == 0:
+            assert mean[j] == -1.0
+            continue
+        m = t.sum() / len(t)
+        assert mean[j] == m
+        np.testing.assert_allclose(sem[j], np.sqrt(max((t * t).sum() / len(t) - m * m, 0.0)
+                                                   / len(t)), rtol=1e-12, atol=1e-9)
+    assert cnt[0] == len(slots) and cnt[4] > 0  # every replica has monomers; some dimers+
