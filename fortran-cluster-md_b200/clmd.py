@@ -177,6 +177,13 @@ class ReplicaResult(C.Structure):
     ]
 
 
+class RatesAcc(C.Structure):
+    """clmd_rates_acc (include/clmd.h): the /CVTPP/ counters of rates()."""
+
+    _fields_ = [("mcts", C.c_double), ("omcts", C.c_double), ("ccn", C.c_int32),
+                ("cen", C.c_int32)]
+
+
 class Request(C.Structure):
     """clmd_request (include/clmd.h)."""
 
@@ -290,6 +297,8 @@ def load(path: str = LIB_PATH):
         "clmd_read_rst": ([P, C.c_char_p, i], C.c_int),
         "clmd_write_csi": ([P, C.c_int32, C.c_char_p, C.c_char_p], C.c_int),
         "clmd_write_fpt": ([P, C.c_char_p], C.c_int),
+        "clmd_rates": ([P, C.c_int32, C.c_int32, C.POINTER(RatesAcc), C.c_char_p, C.c_char_p],
+                       C.c_int),
         "clmd_ens_write_rst": ([P, C.c_int32, C.c_char_p, C.c_int32], C.c_int),
         "clmd_ens_write_fpt": ([P, C.c_int32, C.c_double, C.c_char_p], C.c_int),
         "clmd_ens_upload": ([P, d, d, d, d, d, d], C.c_int),
@@ -535,6 +544,12 @@ class System:
         self._chk(self.lib.clmd_write_csi(self.h, step, os.fsencode(csi_path),
                                           os.fsencode(fsi_path) if fsi_path else None),
                   "write_csi")
+
+    def rates(self, step, ctrat, acc, out, log=None):
+        """rates.f: evaporation/condensation of the largest cluster (appends
+        to out; the size-change lines go to log, None = stdout)."""
+        self._chk(self.lib.clmd_rates(self.h, step, ctrat, C.byref(acc), os.fsencode(out),
+                                      os.fsencode(log) if log else None), "rates")
 
     def write_fpt(self, path):
         """wrt-fpt.f: append the first-passage table."""

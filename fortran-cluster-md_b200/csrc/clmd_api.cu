@@ -265,10 +265,12 @@ extern "C" int clmd_destroy(clmd_system* S) {
                 S->scan_aux, S->partials, S->st, S->parent, S->parent2, S->cl,
                 S->clf, S->cs, S->csf, S->csi, S->csif, S->cgs, S->cgsf, S->cgsa, S->cgsfa,
                 S->cfpt, S->cfptf, S->cek, S->cekf, S->ceks, S->ceksf, S->deg, S->deg1,
-                S->liq, S->liqrank, S->bonds, S->nbonds};
+                S->liq, S->liqrank, S->bonds, S->nbonds, S->r_ocl, S->r_ocs, S->r_ocek,
+                S->r_dev};
   for (void* p : ps)
     if (p) cudaFree(p);
   if (S->h_sc) cudaFreeHost(S->h_sc);
+  if (S->r_host) cudaFreeHost(S->r_host);
   if (S->stream) cudaStreamDestroy(S->stream);
   if (S->side) cudaStreamDestroy(S->side);
   delete S;

@@ -319,6 +319,26 @@ void chk_nucleation_(int32_t* step) {
 
 void chk_nucleation__(int32_t* step) { chk_nucleation_(step); }
 
+// rates.f on the device; unit 67 is the file fxrat names (main.f:49), the
+// counters are the /CVTPP/ ones
+void rates_(int32_t* step) {
+  ensure();
+  if (g_mirror) upload();
+  char path[81];
+  memcpy(path, filep_.fxrat, 80);
+  path[80] = 0;
+  for (int k = 79; k >= 0 && (path[k] == ' ' || path[k] == 0); k--) path[k] = 0;
+  clmd_rates_acc acc = {cvtpp_.mcts, cvtpp_.omcts, cvtpp_.ccn, cvtpp_.cen};
+  int st = clmd_rates(g_sys, *step, cvtpp_.ctrat, &acc, path[0] ? path : nullptr, nullptr);
+  if (st) fatal(st, *step);
+  cvtpp_.mcts = acc.mcts;
+  cvtpp_.omcts = acc.omcts;
+  cvtpp_.ccn = acc.ccn;
+  cvtpp_.cen = acc.cen;
+  publish(*step);
+  download_clusters();
+}
+
 void clmd_f77_reset(void) {
   if (g_sys) clmd_destroy(g_sys);
   g_sys = nullptr;

@@ -52,6 +52,11 @@ struct clmd_system {
   int2* bonds = nullptr;
   unsigned long long* nbonds = nullptr;
   int bond_cap = 0;
+  // rates(): the previous analysis (rates.f's ocs/ocl/ocek) and the picks
+  int *r_ocl = nullptr, *r_ocs = nullptr;
+  double* r_ocek = nullptr;
+  unsigned long long* r_dev = nullptr;  // 2 keys, 2 counts, 2 doubles
+  unsigned long long* r_host = nullptr; // pinned copy
   // launch geometry
   int nblk = 1;          // ceil(N / kBlock)
   int cyc_blocks = 1;    // co-resident blocks of the persistent kernel

@@ -340,6 +340,22 @@ int clmd_write_fpt(clmd_system* sys, const char* path);
  * reference's placeholder). */
 int clmd_ens_write_rst(clmd_ensemble* e, int32_t slot, const char* path, int32_t mxa);
 int clmd_ens_write_fpt(clmd_ensemble* e, int32_t slot, double dt, const char* path);
+/* rates.f:44-100: condensation / evaporation of the largest cluster.  Keeps
+ * the previous analysis's labels, sizes and kinetic energies, runs
+ * stoddard(step) unless this step was analysed already (then the
+ * reference's warning), finds the largest cluster before and after (first
+ * label of the largest size), counts atoms that joined (cn) and left (en)
+ * it, and appends the reference's unit-67 line to out every ctrat steps
+ * (ctrat = 1: every call with cn + en != 0); the write(*,1) line for a
+ * change of size goes to log (NULL: stdout).  acc holds the /CVTPP/
+ * counters the reference keeps across calls (zero them at the start, as
+ * read-3d.f:109-111 does). */
+typedef struct clmd_rates_acc {
+  double mcts, omcts;  /* cvtpp.inc mcts, omcts */
+  int32_t ccn, cen;    /* cvtpp.inc ccn, cen */
+} clmd_rates_acc;
+int clmd_rates(clmd_system* sys, int32_t step, int32_t ctrat, clmd_rates_acc* acc,
+               const char* out, const char* log);
 /* Mean first-passage statistics over the occupied slots, on the device
  * (helpers/passage-time.f + helpers/mpt.f:80-92 in one pass): for each size
  * j = 1..cap, count[j-1] replicas whose largest cluster reached j, the mean

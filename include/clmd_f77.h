@@ -126,6 +126,10 @@ void stopdead_(int32_t* step);       /* stopdead-m.f:10 */
 void stoddard_(int32_t* step);       /* stoddard-pbc-n-m.f:11 / stoddard-pbc-n-m-fre.f:11 */
 void chk_nucleation_(int32_t* step); /* chk-nucleation.f:15 */
 void chk_nucleation__(int32_t* step);/* same, g77 / -fsecond-underscore mangling */
+/* rates.f:12-100 (rates(step), main.f:119 when ftrat != 0): appends to the
+ * file fxrat names; /CVTPP/ ccn, cen, mcts, omcts, ctrat as in the
+ * reference. */
+void rates_(int32_t* step);
 
 /* read-3d.f:11-302 for C/C++ hosts without a Fortran readdata(): parses the
  * .3d deck at path into the common blocks (returns 0 on success). */

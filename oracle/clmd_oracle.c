@@ -36,6 +36,11 @@ struct orc_sys {
   /* NH scratch (int-verlet-nh-mav.f:28-30) */
   double *vxn, *vyn, *vzn, *vxo, *vyo, *vzo, *bx, *by, *bz;
   double *fsx, *fsy, *fsz; /* for-a-lj-n-pbc-m.f:37 */
+  /* rates.f: its local ocs/ocl/ocek and the /CVTPP/ counters */
+  int *ocs, *ocl;
+  double* ocek;
+  int ccn, cen;
+  double mcts, omcts;
 };
 
 static void* xc(size_t n, size_t sz) {
@@ -105,6 +110,11 @@ orc_sys* orc_create(const clmd_config* cfg) {
 }
 
 void orc_destroy(orc_sys* S) {
+  if (S && S->ocs) {
+    free(S->ocs);
+    free(S->ocl);
+    free(S->ocek);
+  }
   if (!S) return;
   void* ps[] = {S->x, S->y, S->z, S->vx, S->vy, S->vz, S->ax, S->ay, S->az, S->api,
                 S->atnlist, S->atnidx, S->cl, S->clf, S->cs, S->csf, S->cc, S->ccf,
@@ -922,6 +932,122 @@ int orc_stoddard(orc_sys* S, int32_t step) {
   if (S->sc.status) return S->sc.status;
   if (S->c.clustering == CLMD_CLU_FRENKEL) return stoddard_frenkel(S, step);
   return stoddard_stillinger(S, step);
+}
+
+/* Fortran's Iw / Fw.d edit descriptors: right-justified, asterisks when
+ * the value does not fit */
+static void fput_i(FILE* f, long long v, int w) {
+  char b[32];
+  int n = snprintf(b, sizeof(b), "%lld", v);
+  if (n > w) {
+    for (int k = 0; k < w; k++) fputc('*', f);
+  } else {
+    fprintf(f, "%*s", w, b);
+  }
+}
+static void fput_f(FILE* f, double v, int w, int d) {
+  char b[64];
+  int n = snprintf(b, sizeof(b), "%.*f", d, v);
+  if (n > w || v != v) {
+    for (int k = 0; k < w; k++) fputc('*', f);
+  } else {
+    fprintf(f, "%*s", w, b);
+  }
+}
+
+/* rates.f:44-100: evaporation / condensation of the largest cluster between
+ * the previous analysis and this step's.  out = unit 67, log = the
+ * write(*,1) lines (NULL: stdout). */
+int orc_rates(orc_sys* S, int32_t step, int32_t ctrat, const char* out, const char* log) {
+  const int N = S->N;
+  if (ctrat < 1) return CLMD_ERR_ARG;
+  if (!S->ocs) {
+    S->ocs = (int*)xc((size_t)N + 1, sizeof(int));
+    S->ocl = (int*)xc((size_t)N + 1, sizeof(int));
+    S->ocek = (double*)xc((size_t)N + 1, sizeof(double));
+  }
+  FILE* lg = log ? fopen(log, "a") : stdout;
+  if (!lg) return CLMD_ERR_ARG;
+  for (int i = 1; i <= N; i++) { /* :44-48 */
+    S->ocs[i] = S->cs[i];
+    S->ocl[i] = S->cl[i];
+    S->ocek[i] = S->cek[i];
+  }
+  if (S->sc.cstep != step) { /* :50-54 */
+    orc_stoddard(S, step);
+  } else {
+    fprintf(lg, " *** WARNING *** No old Stoddard-list !!\n");
+  }
+  int mcs = 0, omcs = 0, mcln = 0, omcln = 0;
+  for (int i = 1; i <= N; i++) { /* :56-67 */
+    if (S->ocs[i] > omcs) {
+      omcs = S->ocs[i];
+      omcln = i;
+    }
+    if (S->cs[i] > mcs) {
+      mcs = S->cs[i];
+      mcln = i;
+    }
+  }
+  int cn = 0, en = 0;
+  for (int i = 1; i <= N; i++) { /* :69-73 */
+    if (S->cl[i] == mcln && S->ocl[i] != omcln) cn = cn + 1;
+    if (S->cl[i] != mcln && S->ocl[i] == omcln) en = en + 1;
+  }
+  if (mcs != omcs) { /* :75-76 */
+    fput_i(lg, step, 12);
+    int v4[4] = {omcs, mcs, omcln, mcln};
+    for (int k = 0; k < 4; k++) {
+      fputs("  ", lg);
+      fput_i(lg, v4[k], 5);
+    }
+    fputs("  ", lg);
+    fput_i(lg, cn, 2);
+    fputs("  ", lg);
+    fput_i(lg, en, 2);
+    fputc('\n', lg);
+  }
+  if (log) fclose(lg);
+  const double cikb = CLMD_CIKB;
+  double mct = S->cek[mcln] / ((double)mcs * 1.5 * cikb); /* :78-81 */
+  S->mcts = S->mcts + mct;
+  double omct = S->ocek[omcln] / ((double)omcs * 1.5 * cikb);
+  S->omcts = S->omcts + omct;
+  S->cen = S->cen + en; /* :83-84 */
+  S->ccn = S->ccn + cn;
+  int write = 0;
+  double c4 = mct, c5 = omct;
+  int c6 = cn, c7 = en;
+  if (ctrat != 1) { /* :85-98 */
+    if (step % ctrat == 0) {
+      write = 1;
+      c4 = S->mcts / (double)(float)ctrat;
+      c5 = S->omcts / (double)(float)ctrat;
+      c6 = S->ccn;
+      c7 = S->cen;
+      S->ccn = 0;
+      S->cen = 0;
+      S->mcts = 0.0;
+    }
+  } else if ((en + cn) != 0) {
+    write = 1;
+  }
+  if (write && out) { /* format 10 */
+    FILE* f = fopen(out, "a");
+    if (!f) return CLMD_ERR_ARG;
+    fput_i(f, step, 12);
+    fputc(' ', f); fput_i(f, omcs, 6);
+    fputc(' ', f); fput_i(f, mcs, 6);
+    fputc(' ', f); fput_f(f, c4, 10, 4);
+    fputc(' ', f); fput_f(f, c5, 10, 4);
+    fputc(' ', f); fput_i(f, c6, 3);
+    fputc(' ', f); fput_i(f, c7, 3);
+    fputc(' ', f); fput_i(f, mcln, 6);
+    fputc(' ', f); fput_i(f, omcln, 6);
+    fputc('\n', f);
+    fclose(f);
+  }
+  return S->sc.status;
 }
 
 /* chk-nucleation.f:15-58 */

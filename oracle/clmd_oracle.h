@@ -46,6 +46,9 @@ int orc_thermostat(orc_sys* S, int32_t step);
 int orc_stopdead(orc_sys* S, int32_t step);
 int orc_stoddard(orc_sys* S, int32_t step);
 int orc_chk_nucleation(orc_sys* S, int32_t* step);
+/* rates.f:44-100 (appends to out, the reference's unit 67; the write(*,1)
+ * lines go to log, NULL = stdout). */
+int orc_rates(orc_sys* S, int32_t step, int32_t ctrat, const char* out, const char* log);
 int orc_run(orc_sys* S, int32_t first, int32_t nsteps, int32_t* next_step);
 
 int orc_get_halflist(orc_sys* S, int32_t* atnlist, int64_t cap, int32_t* atnidx,

@@ -56,6 +56,7 @@ def load():
         "orc_stopdead": ([P, C.c_int32], C.c_int),
         "orc_stoddard": ([P, C.c_int32], C.c_int),
         "orc_chk_nucleation": ([P, i], C.c_int),
+        "orc_rates": ([P, C.c_int32, C.c_int32, C.c_char_p, C.c_char_p], C.c_int),
         "orc_run": ([P, C.c_int32, C.c_int32, i], C.c_int),
         "orc_get_halflist": ([P, i, C.c_int64, i, C.POINTER(C.c_int64)], C.c_int),
         "orc_get_clusters": ([P, C.POINTER(clmd.ClusterView)], C.c_int),
@@ -165,6 +166,11 @@ class Oracle:
         s = C.c_int32(step)
         st = self.lib.orc_chk_nucleation(self.h, C.byref(s))
         return st, s.value
+
+    def rates(self, step, ctrat, out, log=None):
+        """rates.f: appends to out (unit 67); the write(*,1) lines to log."""
+        return self.lib.orc_rates(self.h, step, ctrat, os.fsencode(out),
+                                  os.fsencode(log) if log else None)
 
     def run(self, first, nsteps):
         nxt = C.c_int32(0)

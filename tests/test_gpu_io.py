@@ -2,7 +2,9 @@
 reference's wrt-rst.f record layout, a restart that continues bit-identically,
 and the wrt-csi.f / wrt-csi-fre.f / wrt-fpt.f text formats checked against an
 independent Python restatement of their Fortran edit descriptors."""
+import os
 import struct
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -12,6 +14,8 @@ import orc
 from conftest import random_state, start_pair
 
 pytestmark = pytest.mark.gpu
+
+GOLDEN = Path(os.path.dirname(os.path.abspath(__file__))) / "golden"
 
 
 def read_records(path):
@@ -185,3 +189,44 @@ def test_ensemble_replica_files(gpu, tmp_path):
             + F(float(np.float32(int(np.float32(-1) * rdt)) / rdt), 12, 4)
             for i in range(1, 129) if fpt[i - 1] != -1]
     assert open(tmp_path / "r.fpt").read().splitlines() == want
+
+
+@pytest.mark.parametrize("ctrat", [1, 20])
+def test_rates_match_oracle(gpu, tmp_path, ctrat):
+    """rates.f on the device against the oracle's restatement, both driven in
+    lockstep through main.f's order (rates(i), then the integrator) on the
+    bit-identical FP64 velocity-Verlet trajectory: the unit-67 file and the
+    size-change log agree line for line.  Real units from a deck (argon,
+    Angstrom, K), at a density where the largest cluster changes."""
+    cfg, _, _ = orc.readdata(str(GOLDEN / "nose_vapour.3d"))
+    n = 3000
+    sig = cfg.apsig[0]
+    L = (n / 0.3) ** (1.0 / 3.0) * sig
+    cfg.natom = n
+    cfg.atsorts = 1  # argon only (the deck also has a carrier species)
+    cfg.apnum[0] = n
+    cfg.apnum[1] = 0
+    cfg.boxx = cfg.boxy = cfg.boxz = L
+    cfg.integrator = clmd.INT_VERLET
+    cfg.ethst = b"-"
+    cfg.clustering = clmd.CLU_STILLINGER
+    kt_m = clmd.CIKB * cfg.att / cfg.apmas[0]
+    arrs = clmd.init_random(n, (L, L, L), 0.9 * sig, kt_m, 12)
+    z0 = np.zeros(n)
+    st = clmd.State(*arrs, z0, z0, z0)
+    g = clmd.System(cfg)
+    o = orc.Oracle(cfg)
+    start_pair(g, o, cfg, st)
+    g.stoddard(-1)
+    o.stoddard(-1)
+    acc = clmd.RatesAcc()
+    paths = {k: tmp_path / k for k in ("g.rat", "g.log", "o.rat", "o.log")}
+    for i in range(120):
+        g.rates(i, ctrat, acc, paths["g.rat"], paths["g.log"])
+        o.rates(i, ctrat, str(paths["o.rat"]), str(paths["o.log"]))
+        g.integrator(i)
+        o.integrator(i)
+    rg, ro = open(paths["g.rat"]).read(), open(paths["o.rat"]).read()
+    assert rg == ro
+    assert open(paths["g.log"]).read() == open(paths["o.log"]).read()
+    assert len(rg.splitlines()) > 0

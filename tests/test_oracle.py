@@ -13,7 +13,7 @@ import pytest
 
 import clmd
 import orc
-from conftest import REPO
+from conftest import REPO, random_state
 
 GOLDEN = sorted(glob.glob(os.path.join(REPO, "tests", "golden", "*.json")))
 
@@ -232,3 +232,20 @@ def test_errors_are_statuses_not_stops():
     o2.set_state(clmd.State(x, y, z, vx, vy, vz, 0 * x, 0 * x, 0 * x),
                  scalars=orc.scalars_init(cfg2))
     assert o2.neighbor(0)[0] == clmd.ERR_LIST_OVERFLOW
+
+
+def test_oracle_rates_warning_and_quiet_step(tmp_path):
+    """rates.f:50-54: a step already analysed keeps the old lists (warning),
+    so nothing condensed or evaporated and, with ctrat = 1, no line."""
+    cfg = clmd.lj_config(400, 0.3, 0.7)
+    st = random_state(cfg, 3)
+    o = orc.Oracle(cfg)
+    o.set_state(st, scalars=orc.scalars_init(cfg))
+    o.neighbor(0)
+    o.stoddard(5)
+    out, log = tmp_path / "o.rat", tmp_path / "o.log"
+    assert o.rates(5, 1, str(out), str(log)) == 0
+    assert "No old Stoddard-list" in open(log).read()
+    assert not out.exists()
+    assert o.rates(6, 1, str(out), str(log)) == 0  # same positions: same clusters
+    assert not out.exists()
