@@ -78,7 +78,7 @@ class Config(C.Structure):
         ("apth", C.c_char * MXSORTS),
         ("ethst", C.c_char),
         ("clnuctrl", C.c_char),
-        ("pad", C.c_char * 4),
+        ("forcevar", C.c_char), ("pad", C.c_char * 3),
     ]
 
 
@@ -299,6 +299,7 @@ def load(path: str = LIB_PATH):
         "clmd_write_fpt": ([P, C.c_char_p], C.c_int),
         "clmd_rates": ([P, C.c_int32, C.c_int32, C.POINTER(RatesAcc), C.c_char_p, C.c_char_p],
                        C.c_int),
+        "clmd_thermostat_clu": ([P, C.c_int32, C.c_char, C.c_int32], C.c_int),
         "clmd_ens_write_rst": ([P, C.c_int32, C.c_char_p, C.c_int32], C.c_int),
         "clmd_ens_write_fpt": ([P, C.c_int32, C.c_double, C.c_char_p], C.c_int),
         "clmd_ens_upload": ([P, d, d, d, d, d, d], C.c_int),
@@ -497,6 +498,11 @@ class System:
 
     def thermostat(self, step):
         return self._chk(self.lib.clmd_thermostat(self.h, step), "thermostat")
+
+    def thermostat_clu(self, step, eclth, ecltim):
+        """scalev-clu.f: cluster and gas scaled separately every ecltim."""
+        self._chk(self.lib.clmd_thermostat_clu(self.h, step, eclth.encode(), ecltim),
+                  "thermostat_clu")
 
     def stopdead(self, step):
         return self._chk(self.lib.clmd_stopdead(self.h, step), "stopdead")

@@ -97,6 +97,7 @@ static void fill_params(const clmd_config* c, Params* P) {
   P->ftcsi = c->ftcsi;
   P->integrator = c->integrator;
   P->precision = c->precision == CLMD_PREC_MIXED ? CLMD_PREC_MIXED : CLMD_PREC_FP64;
+  P->r12 = c->forcevar == 'r';
   P->clustering = c->clustering;
   P->ethst = c->ethst;
   P->clnuctrl = c->clnuctrl;
@@ -164,9 +165,12 @@ extern "C" int clmd_create(const clmd_config* cfg, clmd_system** out) {
   P.ncy_max = ny;
   P.ncz_max = nz;
   S->ncell_alloc = nx * ny * nz;
-  long long cap = cfg->nlist_cap > 0 ? cfg->nlist_cap : (long long)N * 64 + (1 << 20);
+  // the full list holds every pair twice; a caller-given atnlist capacity
+  // (headers + half pairs) is enforced with the reference's rule instead
+  long long cap = cfg->nlist_cap > 0 ? 2 * cfg->nlist_cap : (long long)N * 64 + (1 << 20);
   if (cap > 0x7fffffffLL - 1024) cap = 0x7fffffffLL - 1024;
   P.list_cap = (int)cap;
+  P.half_cap = cfg->nlist_cap > 0 ? cfg->nlist_cap : 0;
   S->bond_cap = (int)std::max<long long>(cap / 2, 1024);
   S->nblk = (N + kBlock - 1) / kBlock;
   size_t npart = std::max<size_t>((size_t)S->nblk * 12, (size_t)kMaxRedBlocks * 3) + 64;

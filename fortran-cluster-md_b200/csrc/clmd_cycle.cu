@@ -480,7 +480,11 @@ __device__ bool rebuild(const Params& P, DevState* st, Blk& B, const CycleArgs& 
     A.row_lo[p] = lo;
   }
   if (!gbar(st)) return false;
-  if (__ldcg(&st->err_new) != 0) {
+  // neighbor-pbc-mav.f:95-97: the half list's write cursor after the last
+  // row (1 + natom headers + half pairs) plus natom must stay within mxnlist
+  const bool full = P.half_cap > 0 &&
+                    (long long)(__ldcg(&st->list_used) / 2ull) + 2LL * P.N + 1 > P.half_cap;
+  if (__ldcg(&st->err_new) != 0 || full) {
     if (threadIdx.x == 0 && B.q.status == 0) {
       B.q.status = CLMD_ERR_LIST_OVERFLOW;
       B.q.fail_step = st->cur_step;
@@ -523,9 +527,9 @@ __device__ __forceinline__ Pair pair_forces(const Params& P, DevState* st, const
         raise_err(st, CLMD_ERR_BAD_SPECIES);
         continue;
       }
-      double fij = P.eps[ij] * 48.0 * rij2 * rij6 * (P.c2[ij] * rij6 - P.c3[ij]);
+      double fij = pair_fij(P, ij, rij2, rij6);
       if (own) {
-        r.esum = r.esum + P.eps[ij] * 4.0 * rij6 * (P.c2[ij] * rij6 - P.c1[ij]);
+        r.esum = r.esum + pair_e(P, ij, rij6);
         r.vir = r.vir + fij * r2;
         r.fx = r.fx + fij * dx;
         r.fy = r.fy + fij * dy;
@@ -626,12 +630,12 @@ __device__ __forceinline__ void warp_forces(const Params& P, DevState* st, const
             flag = 2;
           }
         } else {
-          double fij = P.eps[ij] * 48.0 * rij2 * rij6 * (P.c2[ij] * rij6 - P.c3[ij]);
+          double fij = pair_fij(P, ij, rij2, rij6);
           tx = fij * dx;
           ty = fij * dy;
           tz = fij * dz;
           if (own) {
-            esum = esum + P.eps[ij] * 4.0 * rij6 * (P.c2[ij] * rij6 - P.c1[ij]);
+            esum = esum + pair_e(P, ij, rij6);
             vir = vir + fij * r2;
             flag = 1;
           } else {

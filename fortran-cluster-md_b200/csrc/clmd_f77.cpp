@@ -96,6 +96,9 @@ void cfg_from_commons(clmd_config* c) {
   c->integrator = g_integrator;
   c->clustering = g_clustering;
   c->precision = CLMD_PREC_FP64;
+  // for-a-lj-n-pbc-mr.f linked instead of for-a-lj-n-pbc-m.f
+  const char* fv = getenv("CLMD_FORCE");
+  c->forcevar = (fv && strcmp(fv, "mr") == 0) ? 'r' : '-';
 }
 
 void scalars_from_commons(clmd_scalars* q) {
@@ -281,7 +284,11 @@ void integrator_(int32_t* step) {
 void thermostat_(int32_t* step) {
   ensure();
   if (g_mirror) upload();
-  int st = clmd_thermostat(g_sys, *step);
+  // CLMD_THERMOSTAT=clu: scalev-clu.f linked instead of scalev-m.f
+  const char* tv = getenv("CLMD_THERMOSTAT");
+  int st = (tv && strcmp(tv, "clu") == 0)
+               ? clmd_thermostat_clu(g_sys, *step, energ_.eclth, energ_.ecltim)
+               : clmd_thermostat(g_sys, *step);
   if (st) fatal(st, *step);
   publish(*step);
   g_dev_newer = true;

@@ -41,9 +41,11 @@ struct Params {
   int sp_start[CLMD_MXSORTS + 1];  // first atom (0-based) of each species block
   int nbtim, btim, atnenum, csover, clwait, ftcsi;
   int ncx_max, ncy_max, ncz_max;
-  int list_cap;
+  int list_cap;         // full-list entries allocated
+  long long half_cap;   // the caller's atnlist capacity (0: none): the reference's overflow rule
   int integrator, clustering;
   int precision;  // CLMD_PREC_FP64 or CLMD_PREC_MIXED (pair terms)
+  int r12;        // pairs with species 2 purely repulsive (for-a-lj-n-pbc-mr.f)
   char apth[CLMD_MXSORTS];
   char ethst, clnuctrl;
 };
@@ -159,6 +161,19 @@ __device__ __forceinline__ double mimage_bf(double d, double L, double iL, doubl
   return d + L * (bf1 - (double)(int)(bf2 + d * iL));
 }
 
+// LJ pair factor f_ij and energy term (for-a-lj-n-pbc-m.f:113-131); with
+// P.r12 the pairs involving species 2 (ij = 3, 4) are the r^-12 wall of
+// for-a-lj-n-pbc-mr.f:121-127.  Left to right, as the reference's
+// expressions.
+__device__ __forceinline__ double pair_fij(const Params& P, int ij, double rij2, double rij6) {
+  if (P.r12 && ij >= 3) return P.eps[ij] * 12.0 * P.c2[ij] * rij2 * rij6 * rij6;
+  return P.eps[ij] * 48.0 * rij2 * rij6 * (P.c2[ij] * rij6 - P.c3[ij]);
+}
+__device__ __forceinline__ double pair_e(const Params& P, int ij, double rij6) {
+  if (P.r12 && ij >= 3) return P.eps[ij] * P.c2[ij] * rij6 * rij6;
+  return P.eps[ij] * 4.0 * rij6 * (P.c2[ij] * rij6 - P.c1[ij]);
+}
+
 // Mixed-precision pair term (CLMD_PREC_MIXED): the caller has the FP64
 // minimum-image difference and r^2 (the cut-off test stays FP64); the LJ
 // factors, f_ij and the energy and virial terms are FP32.  t* get the FP32
@@ -171,11 +186,12 @@ __device__ __forceinline__ void pair_term_f32(const Params& P, int ij, double r2
   const float r6 = ri2 * ri2 * ri2;
   const float eps = (float)P.eps[ij], c1 = (float)P.c1[ij], c2 = (float)P.c2[ij],
               c3 = (float)P.c3[ij];
-  const float fij = eps * 48.0f * ri2 * r6 * (c2 * r6 - c3);
+  const bool r12 = P.r12 && ij >= 3;
+  const float fij = r12 ? eps * 12.0f * c2 * ri2 * r6 * r6 : eps * 48.0f * ri2 * r6 * (c2 * r6 - c3);
   tx = (double)(fij * (float)dx);
   ty = (double)(fij * (float)dy);
   tz = (double)(fij * (float)dz);
-  e = (double)(eps * 4.0f * r6 * (c2 * r6 - c1));
+  e = (double)(r12 ? eps * c2 * r6 * r6 : eps * 4.0f * r6 * (c2 * r6 - c1));
   w = (double)(fij * r2);
 }
 

@@ -90,9 +90,9 @@ __global__ void __launch_bounds__(kBlock) k_force(Params P, DevState* st, const 
           kahan_add(sz, cz, sg * (float)tz);
           continue;
         }
-        double fij = P.eps[ij] * 48.0 * rij2 * rij6 * (P.c2[ij] * rij6 - P.c3[ij]);
+        double fij = pair_fij(P, ij, rij2, rij6);
         if (own) {
-          esum = esum + P.eps[ij] * 4.0 * rij6 * (P.c2[ij] * rij6 - P.c1[ij]);
+          esum = esum + pair_e(P, ij, rij6);
           vir = vir + fij * r2;
           fx = fx + fij * dx;
           fy = fy + fij * dy;

@@ -1,9 +1,15 @@
-// clmd_rates.cu -- rates(step) (rates.f:44-100): atoms that condensed on or
+// clmd_rates.cu -- the routines that act on the largest cluster.
+//
+// rates(step) (rates.f:44-100): atoms that condensed on or
 // evaporated from the largest cluster between two cluster analyses, on the
 // device: the previous labels are kept, the largest cluster before and after
 // is an atomic max over (size, -label) keys, and the two counts are block
 // reductions; the host keeps the reference's running sums and writes its
 // fixed-format lines.
+//
+// thermostat(step) of scalev-clu.f:41-83: every ecltim steps the biggest
+// cluster and the gas are scaled to the temperature separately, otherwise
+// all atoms with one factor from the current ekin.
 #include <cuda_runtime.h>
 #include <stdio.h>
 
@@ -81,10 +87,105 @@ void put_f(FILE* f, double v, int w, int d) {
     fprintf(f, "%*s", w, b);
 }
 
+// ---- scalev-clu.f: the biggest cluster and the gas scaled separately ------
+__global__ void k_big_key(int n, const int* cs, unsigned long long* key) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long k = 0;
+  if (i < n && cs[i] > 0) k = ((unsigned long long)cs[i] << 32) | (0xffffffffull - i);
+  for (int o = 16; o > 0; o >>= 1) k = max(k, __shfl_xor_sync(0xffffffffu, k, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(key, k);
+}
+
+// per block: sum of cek over the labels other than the biggest one, in a
+// fixed tree (deterministic)
+__global__ void k_gas_ekin(int n, const double* cek, const unsigned long long* key,
+                           double* partials) {
+  __shared__ double sh[kRB / 32];
+  const int ci = key_label(*key) - 1;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v = (i < n && i != ci) ? cek[i] : 0.0;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < kRB / 32; w++) t += sh[w];
+    partials[blockIdx.x] = t;
+  }
+}
+
+// scalev-clu.f:58-59: kfG and kfC from the block sums, added in order
+__global__ void k_clu_factors(Params P, int nb, const double* partials, const int* cs,
+                              const double* cek, const unsigned long long* key, double* kf) {
+  double ekinG = 0.0;
+  for (int b = 0; b < nb; b++) ekinG += partials[b];
+  const int ci = key_label(*key) - 1;
+  const double cikb = CLMD_CIKB;
+  kf[0] = sqrt(1.5 * cikb * P.att * (double)(P.N - cs[ci]) / ekinG);  // gas
+  kf[1] = sqrt(1.5 * cikb * P.att * (double)cs[ci] / cek[ci]);        // cluster
+}
+
+// scalev-clu.f:60-70 (mode 1) or :75-80 (mode 0, one factor for all)
+__global__ void k_clu_scale(Params P, DevState* st, const int* perm, const int* cl, double* vx,
+                            double* vy, double* vz, const double* kf,
+                            const unsigned long long* key, int mode, double ekinT) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p == 0) st->s.ekin = ekinT;  // :82
+  if (p >= P.N) return;
+  double k = kf[0];
+  if (mode == 1 && cl[perm[p]] == key_label(*key)) k = kf[1];
+  vx[p] = vx[p] * k;
+  vy[p] = vy[p] * k;
+  vz[p] = vz[p] * k;
+}
+
 }  // namespace
 }  // namespace clmd
 
 using namespace clmd;
+
+extern "C" int clmd_thermostat_clu(clmd_system* S, int32_t step, char eclth, int32_t ecltim) {
+  if (!S) return CLMD_ERR_ARG;
+  const bool clu = eclth == 'X';
+  if (clu && ecltim <= 0) return CLMD_ERR_ARG;
+  const int n = S->P.N;
+  cudaStream_t st = S->stream;
+  if (!S->r_dev) {
+    if (cudaMalloc(&S->r_dev, 8 * 6) != cudaSuccess ||
+        cudaMallocHost(&S->r_host, 8 * 6) != cudaSuccess) {
+      cudaGetLastError();
+      return CLMD_ERR_NOMEM;
+    }
+  }
+  clmd_scalars q;
+  int rc = clmd_get_scalars(S, &q);
+  if (rc) return rc;
+  const double ekinT = 1.5 * CLMD_CIKB * S->P.att * (double)n;
+  const int nb = (n + kRB - 1) / kRB;
+  unsigned long long* key = S->r_dev;
+  double* kf = (double*)(S->r_dev + 4);
+  int mode = 0;
+  if (clu && step % ecltim == 0) {
+    if (q.cstep != step) {
+      rc = clmd_stoddard(S, step);
+      if (rc) return rc;
+    }
+    mode = 1;
+    cudaMemsetAsync(key, 0, 8, st);
+    k_big_key<<<nb, kRB, 0, st>>>(n, S->cs, key);
+    k_gas_ekin<<<nb, kRB, 0, st>>>(n, S->cek, key, S->partials);
+    k_clu_factors<<<1, 1, 0, st>>>(S->P, nb, S->partials, S->cs, S->cek, key, kf);
+    S->launches += 3;
+  } else {
+    const double k = sqrt(ekinT / q.ekin);  // :75 uses the current ekin
+    cudaMemcpyAsync(kf, &k, 8, cudaMemcpyHostToDevice, st);
+    cudaStreamSynchronize(st);
+  }
+  k_clu_scale<<<nb, kRB, 0, st>>>(S->P, S->st, S->perm, S->cl, S->vx, S->vy, S->vz, kf, key,
+                                   mode, ekinT);
+  S->launches++;
+  return clmd_get_scalars(S, &q);
+}
 
 extern "C" int clmd_rates(clmd_system* S, int32_t step, int32_t ctrat, clmd_rates_acc* acc,
                           const char* out, const char* log) {

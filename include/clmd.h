@@ -81,7 +81,8 @@ typedef struct clmd_config {
   double Q;                   /* Nose-Hoover mass (already * m sigma^2) */
   double boxx, boxy, boxz;    /* periodic box */
   double dt;                  /* time step */
-  int64_t nlist_cap;          /* half-list entry capacity, 0 = automatic */
+  int64_t nlist_cap;          /* atnlist capacity (mxnlist: headers + half pairs); the
+                                 reference's "nearly full" rule applies; 0 = automatic */
   int32_t natom;              /* total atoms */
   int32_t atsorts;            /* species count (1..CLMD_MXSORTS) */
   int32_t apnum[CLMD_MXSORTS];/* atoms per species, contiguous, in order */
@@ -97,7 +98,9 @@ typedef struct clmd_config {
   char apth[CLMD_MXSORTS];    /* 'X' = species thermostatted by velocity scaling */
   char ethst;                 /* 'X' velocity scaling every step, 'N' Nose-Hoover, '-' none */
   char clnuctrl;              /* 'X' = abort the run on nucleation */
-  char pad[4];
+  char forcevar;              /* 'r': pairs with species 2 are the r^-12 wall of
+                                 for-a-lj-n-pbc-mr.f; else LJ (for-a-lj-n-pbc-m.f) */
+  char pad[3];
 } clmd_config;
 
 /* Dynamic scalars: the hot path's scalar members of /ENERG/, /ATOMP/,
@@ -356,6 +359,13 @@ typedef struct clmd_rates_acc {
 } clmd_rates_acc;
 int clmd_rates(clmd_system* sys, int32_t step, int32_t ctrat, clmd_rates_acc* acc,
                const char* out, const char* log);
+/* scalev-clu.f:41-83, the cluster/gas velocity scaling variant of
+ * thermostat(step): when eclth == 'X' and step is a multiple of ecltim
+ * (read-3d.f:176-180), stoddard(step) if not done, then the biggest cluster
+ * (first label of the largest size) is scaled to 1.5 kT per atom and the
+ * rest of the system separately; otherwise every velocity is scaled by
+ * sqrt(ekinT / ekin) with the current ekin.  ekin = ekinT afterwards. */
+int clmd_thermostat_clu(clmd_system* sys, int32_t step, char eclth, int32_t ecltim);
 /* Mean first-passage statistics over the occupied slots, on the device
  * (helpers/passage-time.f + helpers/mpt.f:80-92 in one pass): for each size
  * j = 1..cap, count[j-1] replicas whose largest cluster reached j, the mean

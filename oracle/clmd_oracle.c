@@ -417,6 +417,12 @@ int orc_accatom(orc_sys* S) {
         if (ij == 2) {
           fij = eps11 * 48.0 * rij2 * rij6 * (c112 * rij6 - c113);
           esum = esum + eps11 * 4.0 * rij6 * (c112 * rij6 - c111);
+        } else if (ij == 4 && c->forcevar == 'r') { /* for-a-lj-n-pbc-mr.f:121-123 */
+          fij = eps22 * 12.0 * c222 * rij2 * rij6 * rij6;
+          esum = esum + eps22 * c222 * rij6 * rij6;
+        } else if (ij == 3 && c->forcevar == 'r') { /* for-a-lj-n-pbc-mr.f:125-127 */
+          fij = eps12 * 12.0 * c122 * rij2 * rij6 * rij6;
+          esum = esum + eps12 * c122 * rij6 * rij6;
         } else if (ij == 4) {
           fij = eps22 * 48.0 * rij2 * rij6 * (c222 * rij6 - c223);
           esum = esum + eps22 * 4.0 * rij6 * (c222 * rij6 - c221);
@@ -649,6 +655,49 @@ int orc_thermostat(orc_sys* S, int32_t step) {
     }
     n = n + c->apnum[i - 1];
   }
+  return CLMD_OK;
+}
+
+/* scalev-clu.f:41-83: the biggest cluster and the rest scaled separately
+ * every ecltim steps when eclth == 'X', else one factor from the current
+ * ekin; ekin = ekinT afterwards */
+int orc_thermostat_clu(orc_sys* S, int32_t step, char eclth, int32_t ecltim) {
+  const clmd_config* c = &S->c;
+  clmd_scalars* q = &S->sc;
+  if (q->status) return q->status;
+  const int N = S->N;
+  const double cikb = CLMD_CIKB;
+  double ekinT = 1.5 * cikb * c->att * N;
+  if (eclth == 'X' && ecltim > 0 && step % ecltim == 0) {
+    if (q->cstep != step) orc_stoddard(S, step);
+    int cb = 0, ci = 0;
+    for (int i = 1; i <= N; i++)
+      if (cb < S->cs[i]) {
+        cb = S->cs[i];
+        ci = i;
+      }
+    double ekinG = 0.0;
+    for (int i = 1; i <= N; i++)
+      if (i != ci) ekinG = ekinG + S->cek[i];
+    double kfG = sqrt(1.5 * cikb * c->att * (N - S->cs[ci]) / ekinG);
+    double kfC = sqrt(1.5 * cikb * c->att * S->cs[ci] / S->cek[ci]);
+    for (int i = 1; i <= N; i++) {
+      double k = S->cl[i] == ci ? kfC : kfG;
+      S->vx[i] = S->vx[i] * k;
+      S->vy[i] = S->vy[i] * k;
+      S->vz[i] = S->vz[i] * k;
+    }
+  } else if (eclth == 'X' && ecltim <= 0) {
+    return CLMD_ERR_ARG;
+  } else {
+    double kfG = sqrt(ekinT / q->ekin);
+    for (int i = 1; i <= N; i++) {
+      S->vx[i] = S->vx[i] * kfG;
+      S->vy[i] = S->vy[i] * kfG;
+      S->vz[i] = S->vz[i] * kfG;
+    }
+  }
+  q->ekin = ekinT;
   return CLMD_OK;
 }
 

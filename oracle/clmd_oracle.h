@@ -44,6 +44,8 @@ int orc_zero_acc(orc_sys* S);
 int orc_integrator(orc_sys* S, int32_t step);
 int orc_thermostat(orc_sys* S, int32_t step);
 int orc_stopdead(orc_sys* S, int32_t step);
+/* scalev-clu.f:41-83 (the cluster/gas velocity scaling variant) */
+int orc_thermostat_clu(orc_sys* S, int32_t step, char eclth, int32_t ecltim);
 int orc_stoddard(orc_sys* S, int32_t step);
 int orc_chk_nucleation(orc_sys* S, int32_t* step);
 /* rates.f:44-100 (appends to out, the reference's unit 67; the write(*,1)

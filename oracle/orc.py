@@ -56,6 +56,7 @@ def load():
         "orc_stopdead": ([P, C.c_int32], C.c_int),
         "orc_stoddard": ([P, C.c_int32], C.c_int),
         "orc_chk_nucleation": ([P, i], C.c_int),
+        "orc_thermostat_clu": ([P, C.c_int32, C.c_char, C.c_int32], C.c_int),
         "orc_rates": ([P, C.c_int32, C.c_int32, C.c_char_p, C.c_char_p], C.c_int),
         "orc_run": ([P, C.c_int32, C.c_int32, i], C.c_int),
         "orc_get_halflist": ([P, i, C.c_int64, i, C.POINTER(C.c_int64)], C.c_int),
@@ -158,6 +159,9 @@ class Oracle:
 
     def stopdead(self, step):
         return self.lib.orc_stopdead(self.h, step)
+
+    def thermostat_clu(self, step, eclth, ecltim):
+        return self.lib.orc_thermostat_clu(self.h, step, eclth.encode(), ecltim)
 
     def stoddard(self, step):
         return self.lib.orc_stoddard(self.h, step)

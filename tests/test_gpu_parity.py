@@ -160,3 +160,87 @@ def test_stopdead_thermostat_within_rounding(gpu, two_species):
     for k in ("vx", "vy", "vz"):
         np.testing.assert_allclose(getattr(a, k), getattr(b, k), rtol=1e-13, atol=1e-15)
     assert rel(g.scalars().ekin, o.scalars().ekin) < RTOL_SUM
+
+
+@pytest.mark.parametrize("precision", [clmd.PREC_FP64, clmd.PREC_MIXED])
+def test_repulsive_carrier_variant(gpu, precision):
+    """for-a-lj-n-pbc-mr.f: pairs with species 2 are the r^-12 wall.  FP64:
+    accelerations bit-exact and 50 velocity-Verlet steps bit-identical to
+    the oracle; mixed: forces within 1e-5."""
+    sp = dict(n=1500, sigma=0.758, eps=0.085, mass=0.1)
+    cfg = clmd.lj_config(4000, 0.2, 0.7, species=sp, precision=precision,
+                         nlist_cap=4000 * 80)
+    cfg.forcevar = b"r"
+    g, o = pair(cfg, 8)
+    a, b = g.get_state(), o.get_state()
+    if precision == clmd.PREC_FP64:
+        assert_state_equal(a, b, "forces")
+        for step in range(1, 51):
+            g.integrator(step)
+            o.integrator(step)
+        assert g.scalars().status == 0 and o.scalars().status == 0
+        assert g.scalars().nrebuild == o.scalars().nrebuild > 1
+        assert_state_equal(g.get_state(), o.get_state(), "after 50 steps")
+        assert rel(g.scalars().epot, o.scalars().epot) < RTOL_SUM
+    else:
+        fa = np.stack([a.ax, a.ay, a.az], 1)
+        fb = np.stack([b.ax, b.ay, b.az], 1)
+        assert np.linalg.norm(fa - fb) / np.linalg.norm(fb) <= 1e-5
+    # and it is not the LJ path: the plain config gives other forces
+    cfg2 = clmd.lj_config(4000, 0.2, 0.7, species=sp, nlist_cap=4000 * 80)
+    o2 = orc.Oracle(cfg2)
+    o2.set_state(o.get_state(), scalars=orc.scalars_init(cfg2))
+    o2.neighbor(0)
+    o2.zero_acc()
+    o2.accatom()
+    assert not np.array_equal(o2.get_state().ax, b.ax)
+
+
+@pytest.mark.parametrize("step", [100, 7])
+def test_cluster_thermostat_variant(gpu, step):
+    """scalev-clu.f: at a multiple of ecltim the biggest cluster and the gas
+    get their own factors (their sums in another order: 1e-13); otherwise one
+    factor from the current ekin (bit-exact)."""
+    cfg = clmd.lj_config(3000, 0.3, 0.7)
+    g, o = pair(cfg, 13)
+    for s_ in (g, o):
+        s_.stoddard(step - 1)
+        s_.thermostat_clu(step, "X", 50)
+    a, b = g.get_state(), o.get_state()
+    for k in ("vx", "vy", "vz"):
+        if step % 50 == 0:
+            np.testing.assert_allclose(getattr(a, k), getattr(b, k), rtol=1e-13, atol=1e-15)
+        else:
+            assert np.array_equal(getattr(a, k), getattr(b, k)), k
+    ekinT = 1.5 * clmd.CIKB * cfg.att * cfg.natom
+    assert g.scalars().ekin == ekinT and o.scalars().ekin == ekinT
+    if step % 50 == 0:
+        cg, co = g.clusters(), o.clusters()
+        assert np.array_equal(cg["cl"], co["cl"])
+        big = np.argmax(np.bincount(cg["cl"]))
+        m = cg["cl"] == big
+        v2 = a.vx ** 2 + a.vy ** 2 + a.vz ** 2
+        # the cluster now carries 1.5 kT per atom
+        assert abs(0.5 * v2[m].sum() / (1.5 * clmd.CIKB * cfg.att * m.sum()) - 1) < 1e-12
+
+
+def test_list_capacity_rule_matches_reference(gpu):
+    """neighbor-pbc-mav.f:95-97 stops when the half list's cursor plus natom
+    passes mxnlist: at the exact capacity the engine and the oracle both
+    build the list, one entry less and both report the overflow."""
+    cfg = clmd.lj_config(3000, 0.1, 0.7, nlist_cap=3000 * 100)
+    st = random_state(cfg, 19)
+    o = orc.Oracle(cfg)
+    o.set_state(st, scalars=orc.scalars_init(cfg))
+    o.neighbor(0)
+    need = 2 * 3000 + 1 + o.scalars().npairs_half
+    for cap, want in ((need, 0), (need - 1, clmd.ERR_LIST_OVERFLOW)):
+        c = clmd.lj_config(3000, 0.1, 0.7, nlist_cap=cap)
+        g = clmd.System(c)
+        g.set_state(st, scalars=clmd.scalars_init(c))
+        g.neighbor(0)
+        o2 = orc.Oracle(c)
+        o2.set_state(st, scalars=orc.scalars_init(c))
+        assert o2.neighbor(0)[0] == want
+        assert g.scalars().status == want, (cap, need)
+        g.close()
