@@ -23,9 +23,11 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -973,6 +975,13 @@ struct clmd_ensemble {
   int cls_threads[kClasses] = {128, 256, 512, 1024};
   cudaStream_t cstream[kClasses] = {};
   cudaEvent_t ev0[kClasses] = {}, ev1[kClasses] = {}, evj = nullptr;
+  cudaEvent_t evdone[kClasses] = {};  // join of each class stream
+  // the window launch sequence replayed from a CUDA graph while the
+  // replicas, their classes and the launch shapes stay the same
+  bool use_graphs = true;
+  std::map<void*, size_t> attr_smem;  // dynamic shared memory limit set per kernel
+  cudaGraphExec_t gexec = nullptr;
+  std::vector<long long> gkey;
   float last_ms[kClasses] = {};
   long long last_atoms[kClasses] = {};
   bool tuned = false;
@@ -1038,9 +1047,14 @@ extern "C" int clmd_ens_create(const clmd_ens_config* cfg, clmd_ensemble** out) 
     ECK(cudaStreamCreateWithFlags(&E->cstream[c], cudaStreamNonBlocking));
     ECK(cudaEventCreate(&E->ev0[c]));
     ECK(cudaEventCreate(&E->ev1[c]));
+    ECK(cudaEventCreateWithFlags(&E->evdone[c], cudaEventDisableTiming));
     if (cfg->threads > 0) E->cls_threads[c] = cfg->threads;
   }
   ECK(cudaEventCreateWithFlags(&E->evj, cudaEventDisableTiming));
+  {
+    const char* g = getenv("CLMD_ENS_GRAPHS");
+    E->use_graphs = !(g && g[0] == '0');
+  }
   E->tuned = cfg->threads > 0;
   const long long P = cfg->max_atoms;
   Args& A = E->A;
@@ -1111,8 +1125,10 @@ extern "C" int clmd_ens_destroy(clmd_ensemble* E) {
     if (E->cstream[c]) cudaStreamDestroy(E->cstream[c]);
     if (E->ev0[c]) cudaEventDestroy(E->ev0[c]);
     if (E->ev1[c]) cudaEventDestroy(E->ev1[c]);
+    if (E->evdone[c]) cudaEventDestroy(E->evdone[c]);
   }
   if (E->evj) cudaEventDestroy(E->evj);
+  if (E->gexec) cudaGraphExecDestroy(E->gexec);
   delete E;
   return CLMD_OK;
 }
@@ -1260,10 +1276,19 @@ static EnsKernel kernel_for(int nt, bool sm, bool mixed) {
   }
 }
 
-// one launch of one size class: every listed replica advances by nwin
-// windows; items[] is the class's slice of the device item list
-static int launch_class(clmd_ensemble* E, int c, int item0, int nitems, const int* slots,
-                        int nwin, int nt, bool balanced) {
+// the launch shape of one size class: kernel, dynamic shared memory, grid
+struct ClassLaunch {
+  EnsKernel k = nullptr;
+  size_t smem = 0;
+  int grid = 0, nt = 0, ncmax = 1, item0 = 0, nitems = 0;
+};
+
+static int prepare_class(clmd_ensemble* E, int item0, int nitems, const int* slots, int nt,
+                         ClassLaunch& L) {
+  L = ClassLaunch();
+  L.item0 = item0;
+  L.nitems = nitems;
+  L.nt = nt;
   if (nitems == 0) return CLMD_OK;
   const bool mixed = E->cfg.precision == CLMD_PREC_MIXED;
   // positions stay in shared memory if every replica of the class fits
@@ -1272,33 +1297,46 @@ static int launch_class(clmd_ensemble* E, int c, int item0, int nitems, const in
     const Rep& R = E->h_reps[slots[k]];
     if (smem_bytes(R.natom, R.ncmax, true) + 8192 > E->smem_cap) sm = false;
   }
-  size_t smem = 0;
-  int ncmax = 1;
   for (int k = 0; k < nitems; k++) {
     const Rep& R = E->h_reps[slots[k]];
-    smem = std::max(smem, smem_bytes(R.natom, R.ncmax, sm));
-    ncmax = std::max(ncmax, R.ncmax);
+    L.smem = std::max(L.smem, smem_bytes(R.natom, R.ncmax, sm));
+    L.ncmax = std::max(L.ncmax, R.ncmax);
   }
-  EnsKernel k = kernel_for(nt, sm, mixed);
-  ECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  L.k = kernel_for(nt, sm, mixed);
+  // the attribute only grows: classes that share a kernel may launch it
+  // with different amounts in one sequence (occupancy follows each launch)
+  size_t& lim = E->attr_smem[(void*)L.k];
+  if (L.smem > lim) {
+    ECK(cudaFuncSetAttribute(L.k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
+    lim = L.smem;
+  }
   int per_sm = 0;
-  ECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, nt, smem));
+  ECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, L.k, nt, L.smem));
   if (per_sm < 1) return CLMD_ERR_ARG;
-  int grid = (int)std::min<long long>((long long)per_sm * E->nsm, (long long)nitems);
+  L.grid = (int)std::min<long long>((long long)per_sm * E->nsm, (long long)nitems);
+  return CLMD_OK;
+}
+
+// one launch of one size class on its stream: every listed replica advances
+// by nwin windows (or its balanced step count)
+static int enqueue_class(clmd_ensemble* E, int c, const ClassLaunch& L, int nwin, bool balanced,
+                         bool capturing) {
   cudaStream_t st = E->cstream[c];
   ECK(cudaMemsetAsync(E->d_ctr + c, 0, sizeof(int), st));
   Args A = E->A;
-  A.items = E->d_items + item0;
-  A.iwin = balanced ? E->d_iwin + item0 : nullptr;
+  A.items = E->d_items + L.item0;
+  A.iwin = balanced ? E->d_iwin + L.item0 : nullptr;
   A.ctr = E->d_ctr + c;
-  A.nitems = nitems;
+  A.nitems = L.nitems;
   A.nwin = nwin;
-  A.ncmax = ncmax;
-  ECK(cudaEventRecord(E->ev0[c], st));
-  k<<<grid, nt, smem, st>>>(A);
-  ECK(cudaEventRecord(E->ev1[c], st));
-  E->launches++;
-  return ck(cudaGetLastError(), "k_ens launch");
+  A.ncmax = L.ncmax;
+  const unsigned fl = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+  ECK(cudaEventRecordWithFlags(E->ev0[c], st, fl));
+  L.k<<<L.grid, L.nt, L.smem, st>>>(A);
+  ECK(cudaGetLastError());
+  ECK(cudaEventRecordWithFlags(E->ev1[c], st, fl));
+  ECK(cudaEventRecord(E->evdone[c], st));
+  return CLMD_OK;
 }
 
 // all running replicas, split by size class, each class largest first; the
@@ -1339,35 +1377,83 @@ static int launch_all(clmd_ensemble* E, int nwin, const int* threads, float min_
                         E->stream));
   }
   if (total == 0) return CLMD_OK;
-  ECK(cudaMemcpyAsync(E->d_items, E->h_items, sizeof(int) * total, cudaMemcpyHostToDevice,
-                      E->stream));
-  ECK(cudaEventRecord(E->evj, E->stream));
-  int off = 0;
-  for (int c = 0; c < clmd_ensemble::kClasses; c++) {
-    E->last_atoms[c] = 0;
-    for (int s : cls[c]) E->last_atoms[c] += E->h_reps[s].natom;
-    if (!cls[c].empty()) {
+  ClassLaunch L[clmd_ensemble::kClasses];
+  std::vector<long long> key;
+  key.reserve(total + 64);
+  key.push_back(total);
+  key.push_back(nwin);
+  key.push_back(balanced);
+  for (int k = 0; k < total; k++) key.push_back(E->h_items[k]);
+  {
+    int off = 0;
+    for (int c = 0; c < clmd_ensemble::kClasses; c++) {
+      E->last_atoms[c] = 0;
+      for (int s : cls[c]) E->last_atoms[c] += E->h_reps[s].natom;
+      int st = prepare_class(E, off, (int)cls[c].size(), cls[c].data(), threads[c], L[c]);
+      if (st) return st;
+      key.push_back(L[c].nt);
+      key.push_back(L[c].grid);
+      key.push_back((long long)L[c].smem);
+      key.push_back((long long)(size_t)L[c].k);
+      off += (int)cls[c].size();
+    }
+  }
+  // the sequence: item list (+ balanced step counts) in, the classes on their
+  // streams, per-slot timings and summaries out
+  auto enqueue = [&](bool capturing) -> int {
+    if (balanced)
+      ECK(cudaMemcpyAsync(E->d_iwin, E->h_iwin, sizeof(int) * total, cudaMemcpyHostToDevice,
+                          E->stream));
+    ECK(cudaMemcpyAsync(E->d_items, E->h_items, sizeof(int) * total, cudaMemcpyHostToDevice,
+                        E->stream));
+    ECK(cudaEventRecord(E->evj, E->stream));
+    for (int c = 0; c < clmd_ensemble::kClasses; c++) {
+      if (L[c].nitems == 0) continue;
       ECK(cudaStreamWaitEvent(E->cstream[c], E->evj, 0));
-      int st = launch_class(E, c, off, (int)cls[c].size(), cls[c].data(), nwin, threads[c],
-                            balanced);
+      int st = enqueue_class(E, c, L[c], nwin, balanced, capturing);
       if (st) return st;
     }
-    off += (int)cls[c].size();
-  }
-  for (int c = 0; c < clmd_ensemble::kClasses; c++) {
-    if (cls[c].empty()) {
-      E->last_ms[c] = -1.0f;
-      continue;
+    for (int c = 0; c < clmd_ensemble::kClasses; c++)
+      if (L[c].nitems) ECK(cudaStreamWaitEvent(E->stream, E->evdone[c], 0));
+    ECK(cudaMemcpyAsync(E->h_wtime, E->A.wtime, sizeof(float) * E->cfg.max_replicas,
+                        cudaMemcpyDeviceToHost, E->stream));
+    ECK(cudaMemcpyAsync(E->h_summary, E->A.summary, sizeof(int4) * E->cfg.max_replicas,
+                        cudaMemcpyDeviceToHost, E->stream));
+    return CLMD_OK;
+  };
+  if (E->use_graphs) {
+    if (!E->gexec || key != E->gkey) {
+      if (E->gexec) cudaGraphExecDestroy(E->gexec);
+      E->gexec = nullptr;
+      E->gkey.clear();
+      ECK(cudaStreamBeginCapture(E->stream, cudaStreamCaptureModeThreadLocal));
+      int st = enqueue(true);
+      cudaGraph_t g = nullptr;
+      cudaError_t ce = cudaStreamEndCapture(E->stream, &g);
+      if (st) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+      }
+      ECK(ce);
+      ce = cudaGraphInstantiate(&E->gexec, g, 0);
+      cudaGraphDestroy(g);
+      ECK(ce);
+      E->gkey = key;
     }
-    ECK(cudaStreamWaitEvent(E->stream, E->ev1[c], 0));
+    ECK(cudaGraphLaunch(E->gexec, E->stream));
+  } else {
+    int st = enqueue(false);
+    if (st) return st;
   }
-  ECK(cudaMemcpyAsync(E->h_wtime, E->A.wtime, sizeof(float) * E->cfg.max_replicas,
-                      cudaMemcpyDeviceToHost, E->stream));
-  ECK(cudaMemcpyAsync(E->h_summary, E->A.summary, sizeof(int4) * E->cfg.max_replicas,
-                      cudaMemcpyDeviceToHost, E->stream));
-  ECK(cudaStreamSynchronize(E->stream));
   for (int c = 0; c < clmd_ensemble::kClasses; c++)
-    if (!cls[c].empty()) ECK(cudaEventElapsedTime(&E->last_ms[c], E->ev0[c], E->ev1[c]));
+    if (L[c].nitems) E->launches++;
+  ECK(cudaStreamSynchronize(E->stream));
+  for (int c = 0; c < clmd_ensemble::kClasses; c++) {
+    if (L[c].nitems)
+      ECK(cudaEventElapsedTime(&E->last_ms[c], E->ev0[c], E->ev1[c]));
+    else
+      E->last_ms[c] = -1.0f;
+  }
   E->reps_stale = true;
   return CLMD_OK;
 }

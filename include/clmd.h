@@ -273,7 +273,10 @@ int clmd_ens_add(clmd_ensemble* e, const clmd_replica_spec* spec, const double* 
                  const double* y, const double* z, const double* vx, const double* vy,
                  const double* vz, int32_t* slot);
 /* Advances every running replica by up to nwin windows of ftcsi steps (one
- * persistent launch per size class); replicas stop when done. */
+ * persistent launch per size class, the classes concurrently); replicas stop
+ * when done.  The launch sequence is captured once into a CUDA graph and
+ * replayed while the set of running replicas and the launch shapes stay the
+ * same (CLMD_ENS_GRAPHS=0 in the environment at creation: direct launches). */
 int clmd_ens_step(clmd_ensemble* e, int32_t nwin);
 /* Balanced step for mixed sizes: every running replica advances for about
  * ms of device time (at least one MD step), from the time per step the

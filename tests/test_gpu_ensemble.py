@@ -307,3 +307,40 @@ def test_mean_first_passage_matches_per_replica_tables(gpu):
         np.testing.assert_allclose(sem[j], np.sqrt(max((t * t).sum() / len(t) - m * m, 0.0)
                                                    / len(t)), rtol=1e-12, atol=1e-9)
     assert cnt[0] == len(slots) and cnt[4] > 0  # every replica has monomers; some dimers+
+
+
+def test_graph_replay_same_as_direct_launches(gpu, monkeypatch):
+    """The window sequence replayed from a CUDA graph (default) and issued
+    launch by launch (CLMD_ENS_GRAPHS=0) give bit-identical replicas, also
+    across a membership change (a replica finishing).  (Balanced steps are
+    left out: how many steps they run depends on measured times.)"""
+    rng = np.random.default_rng(5)
+    specs = [(int(rng.integers(200, 6000)), float(rng.uniform(0.02, 0.05)), 600 + k)
+             for k in range(24)]
+
+    def run():
+        e = clmd.Ensemble(clmd.ens_config(sum(n for n, _, _ in specs), 32, ftcsi=20,
+                                          threads=256))
+        slots = []
+        for k, (n, rho, sd) in enumerate(specs):
+            box, arrs = replica_inputs(n, rho, 0.7, sd)
+            slots.append(e.add(n, box, 0.7, *arrs, csover=10**6, budget=60 if k == 3 else 400))
+        for _ in range(4):
+            e.step(1)  # replica 3 finishes after 3 windows: the launch set changes
+        e.step(3)
+        ms, _ = e.last_ms()
+        assert max(ms) > 0
+        return e, slots
+
+    monkeypatch.setenv("CLMD_ENS_GRAPHS", "0")
+    a, sa = run()
+    monkeypatch.delenv("CLMD_ENS_GRAPHS")
+    b, sb = run()
+    for p, q in zip(sa, sb):
+        ra, rb = a.results()[p], b.results()[q]
+        assert (ra.step, ra.done, ra.psi, ra.ekin) == (rb.step, rb.done, rb.psi, rb.ekin)
+        xa, _ = a.state(p)
+        xb, _ = b.state(q)
+        for k in ("x", "vx", "az"):
+            assert np.array_equal(getattr(xa, k), getattr(xb, k)), k
+    assert a.results()[sa[3]].done == 2
