@@ -298,40 +298,65 @@ def pinned(n, torch):
     return torch.empty(n, dtype=torch.float64).pin_memory()
 
 
+class Ranks:
+    """One process per GPU, launched by torchrun (RANK / WORLD_SIZE /
+    LOCAL_RANK / MASTER_* from the environment).  The path has no exchange:
+    ranks run independent replicas (seed + 1000 * rank) and meet only for the
+    timing barrier and the max / sum of their numbers.  backend "nccl" on
+    GPUs; "gloo" runs the same logic on CPU processes."""
+
+    def __init__(self, backend="nccl", timeout_s=300):
+        import torch
+        self.torch = torch
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.dist = self.world > 1
+        self.cuda = backend == "nccl"
+        if self.cuda:
+            torch.cuda.set_device(self.local if self.dist else 0)
+        if self.dist:
+            import datetime
+            torch.distributed.init_process_group(
+                backend, timeout=datetime.timedelta(seconds=timeout_s))
+
+    @property
+    def device(self):
+        return self.local if self.dist else 0
+
+    def barrier(self):
+        if self.dist:
+            self.torch.distributed.barrier()
+        if self.cuda:
+            self.torch.cuda.synchronize()
+
+    def _reduce(self, x, op):
+        if not self.dist:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64,
+                              device="cuda" if self.cuda else "cpu")
+        self.torch.distributed.all_reduce(t, op=op)
+        return float(t.item())
+
+    def max(self, x):
+        return self._reduce(x, self.torch.distributed.ReduceOp.MAX if self.dist else None)
+
+    def sum(self, x):
+        return self._reduce(x, self.torch.distributed.ReduceOp.SUM if self.dist else None)
+
+    def close(self):
+        if self.dist:
+            self.torch.distributed.barrier()
+            self.torch.distributed.destroy_process_group()
+
+
 def engine_arm(args, w):
     import torch
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = world > 1
-    if dist:
-        import datetime
-        import torch.distributed as td
-        torch.cuda.set_device(local)
-        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
-    dev = local if dist else 0
-    torch.cuda.set_device(dev)
+    rk = Ranks(timeout_s=180)
+    rank, world, dist, dev = rk.rank, rk.world, rk.dist, rk.device
     clmd.set_device(dev)
-
-    def barrier():
-        if dist:
-            torch.distributed.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.SUM)
-        return float(t.item())
+    barrier, max_over_ranks, sum_over_ranks = rk.barrier, rk.max, rk.sum
 
     n = w["natom"]
     cyc = w["ftcsi"]
@@ -448,9 +473,7 @@ def engine_arm(args, w):
         }
         print(json.dumps(line), flush=True)
     g.close()
-    if dist:
-        torch.distributed.barrier()
-        torch.distributed.destroy_process_group()
+    rk.close()
 
 
 # ---------------------------------------------------------------------------
@@ -636,30 +659,10 @@ def mixed_force_error(e, slots, specs_by_slot, nsample=3):
 def batched_arm(args):
     import torch
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = world > 1
-    if dist:
-        import datetime
-        import torch.distributed as td
-        torch.cuda.set_device(local)
-        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    dev = local if dist else 0
-    torch.cuda.set_device(dev)
+    rk = Ranks(timeout_s=300)
+    rank, world, dev = rk.rank, rk.world, rk.device
     clmd.set_device(dev)
-
-    def barrier():
-        if dist:
-            torch.distributed.barrier()
-        torch.cuda.synchronize()
-
-    def reduce(x, op):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=op)
-        return float(t.item())
+    barrier = rk.barrier
 
     specs = ensemble_specs(args.replicas, ENSEMBLE["seed"] + 1000 * rank)
     total = sum(sp[0] for sp in specs)
@@ -702,8 +705,8 @@ def batched_arm(args):
     barrier()
     res = e.results()
     atom_steps = sum(slots[k][0] * (res[k].step - r0[k]) for k in slots)
-    el_max = reduce(el, torch.distributed.ReduceOp.MAX if dist else None)
-    units = reduce(float(atom_steps), torch.distributed.ReduceOp.SUM if dist else None)
+    el_max = rk.max(el)
+    units = rk.sum(float(atom_steps))
     value = units / el_max
     launches = e.launches() - l0
 
@@ -726,9 +729,8 @@ def batched_arm(args):
     e2e_s = time.perf_counter() - t
     barrier()
     res = e.results()
-    e2e_units = reduce(float(sum(slots[k][0] * (res[k].step - re0[k]) for k in slots)),
-                       torch.distributed.ReduceOp.SUM if dist else None)
-    e2e_value = e2e_units / reduce(e2e_s, torch.distributed.ReduceOp.MAX if dist else None)
+    e2e_units = rk.sum(float(sum(slots[k][0] * (res[k].step - re0[k]) for k in slots)))
+    e2e_value = e2e_units / rk.max(e2e_s)
     h2d = 6 * 8 * total
     d2h = 6 * 8 * total + 16 * len(slots)
 
@@ -774,9 +776,7 @@ def batched_arm(args):
         }
         print(json.dumps(line), flush=True)
     e.close()
-    if dist:
-        torch.distributed.barrier()
-        torch.distributed.destroy_process_group()
+    rk.close()
 
 
 # served solves: Poisson arrivals, continuous batching (clmd_serve)
@@ -822,17 +822,8 @@ def served_config_json(args, nreq, pool, ngpu):
 def served_arm(args):
     import torch
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = world > 1
-    if dist:
-        import datetime
-        import torch.distributed as td
-        torch.cuda.set_device(local)
-        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    dev = local if dist else 0
-    torch.cuda.set_device(dev)
+    rk = Ranks(timeout_s=600)
+    rank, world, dev = rk.rank, rk.world, rk.device
     clmd.set_device(dev)
     free, _ = torch.cuda.mem_get_info(dev)
     pool = int(min(args.pool_fraction * free / POOL_BYTES_PER_ATOM, 2**31 - 1))
@@ -846,8 +837,7 @@ def served_arm(args):
         r.arrival = 0.0
         r.budget = 400
     e.serve(warm, 30.0)
-    if dist:
-        torch.distributed.barrier()
+    rk.barrier()
     clocks = Clocks(dev)
     l0 = e.launches()
     clocks.start()
@@ -855,17 +845,8 @@ def served_arm(args):
     clk = clocks.stop()
     launches = e.launches() - l0
 
-    def red(x, op):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=op)
-        return float(t.item())
-
-    SUM = torch.distributed.ReduceOp.SUM if dist else None
-    MAX = torch.distributed.ReduceOp.MAX if dist else None
-    wall = red(st.wall, MAX)
-    units = red(st.atom_steps, SUM)
+    wall = rk.max(st.wall)
+    units = rk.sum(st.atom_steps)
     value = units / wall
     if rank == 0:
         lat = np.array([o.finished - o.arrival for o in out if o.done in (1, 2)])
@@ -912,9 +893,7 @@ def served_arm(args):
         }
         print(json.dumps(line), flush=True)
     e.close()
-    if dist:
-        torch.distributed.barrier()
-        torch.distributed.destroy_process_group()
+    rk.close()
 
 
 def served_reference_arm(args):
