@@ -126,7 +126,7 @@ __device__ __forceinline__ double get_max(const double* buf, int slot, double* s
 // ---------------------------------------------------------------------------
 
 // neighbor-pbc-mav.f:48-60, 101-105 and the cell grid
-__device__ void prologue(const Params& P, Blk& B, int step) {
+static __device__ void prologue(const Params& P, Blk& B, int step) {
   clmd_scalars& q = B.q;
   if (q.dmms > (q.atrskin - P.atrcut)) {  // :48-51
     if (q.status == 0) {
@@ -176,7 +176,7 @@ __device__ void prologue(const Params& P, Blk& B, int step) {
 }
 
 // int-verlet-mav.f:64-74 / int-verlet-nh-mav.f:70-78
-__device__ void skin(const Params& P, Blk& B, double dmmr, int step) {
+static __device__ void skin(const Params& P, Blk& B, double dmmr, int step) {
   clmd_scalars& q = B.q;
   dmmr = 2.2 * sqrt(dmmr);
   q.dmms = q.dmms + dmmr;
@@ -280,7 +280,7 @@ struct CycleArgs {
 };
 
 // returns false if the grid must stop (error)
-__device__ bool rebuild(const Params& P, DevState* st, Blk& B, const CycleArgs& A,
+static __device__ bool rebuild(const Params& P, DevState* st, Blk& B, const CycleArgs& A,
                         double4* pos, double* sh) {
   const int N = P.N;
   const int G = gridDim.x * blockDim.x;
@@ -555,6 +555,7 @@ struct WarpStage {
   int flag[32];  // 0 nothing, 1 add, 2 subtract
 };
 
+template <bool MIXED>
 __device__ __forceinline__ void warp_forces(const Params& P, DevState* st, const double4* pos,
                                             const int* list, int st0, int len, int lo,
                                             const double4& pa, double bf1, double bf2,
@@ -572,7 +573,7 @@ __device__ __forceinline__ void warp_forces(const Params& P, DevState* st, const
   e -= len;  // exclusive prefix: this lane's row starts at wbase + e
   const int wbase = __shfl_sync(FULL, st0, 0);
   const int sa = (int)pa.w;
-  const bool mixed = P.precision == CLMD_PREC_MIXED;
+  constexpr bool mixed = MIXED;
   float sx = 0.f, sy = 0.f, sz = 0.f, kx = 0.f, ky = 0.f, kz = 0.f;  // mixed: Kahan sums
   fx = 0.0;
   fy = 0.0;
@@ -689,7 +690,7 @@ __device__ __forceinline__ int sp_block(const Params& P, int ref) {
 enum { SLOT_MAX = 0, SLOT_SUMV2 = 1, SLOT_EPOT = 2, SLOT_VIR = 3, SLOT_EKIN = 4,
        SLOT_DELPS = 5, SLOT_NR = 6, SLOT_EK0 = 6 /* ek per species: 6..15 */ };
 
-template <bool NH, bool THERMO>
+template <bool NH, bool THERMO, bool MIXED>
 __global__ void __launch_bounds__(kPB, CLMD_CYCLE_MINB) k_cycle(Params P, DevState* st,
                                                                 CycleArgs A, int nsteps,
                                                                 int mode) {
@@ -854,7 +855,7 @@ __global__ void __launch_bounds__(kPB, CLMD_CYCLE_MINB) k_cycle(Params P, DevSta
           Pair f;
           f.esum = 0.0;
           f.vir = 0.0;
-          warp_forces(P, st, pos, A.list, act ? A.row_start[p] : 0, act ? A.row_len[p] : 0,
+          warp_forces<MIXED>(P, st, pos, A.list, act ? A.row_start[p] : 0, act ? A.row_len[p] : 0,
                       act ? A.row_lo[p] : 0, pa, bf1, bf2, f.fx, f.fy, f.fz, f.esum, f.vir, W);
           // lanes past N still evaluated pair terms of their warp's atoms
           esum = esum + f.esum;
@@ -1061,6 +1062,19 @@ done:
   }
 }
 
+// This file is compiled twice: as is (the FP64 kernels and the host side)
+// and with CLMD_CYCLE_MIXED (the mixed-precision kernels only).  In one
+// translation unit the two sets got larger local frames and ran ~4% slower.
+typedef void (*CycleKernel)(Params, DevState*, CycleArgs, int, int);
+
+#ifdef CLMD_CYCLE_MIXED
+CycleKernel cycle_kernel_mixed(bool nh, bool th) {
+  if (nh) return th ? k_cycle<true, true, true> : k_cycle<true, false, true>;
+  return th ? k_cycle<false, true, true> : k_cycle<false, false, true>;
+}
+#else
+CycleKernel cycle_kernel_mixed(bool nh, bool th);
+
 static CycleArgs cycle_args(clmd_system* S) {
   CycleArgs A;
   A.pos0 = S->pos;
@@ -1080,12 +1094,11 @@ static CycleArgs cycle_args(clmd_system* S) {
   return A;
 }
 
-typedef void (*CycleKernel)(Params, DevState*, CycleArgs, int, int);
-
 static CycleKernel cycle_kernel(const clmd_system* S) {
   bool nh = S->P.integrator == CLMD_INT_NOSE, th = S->P.ethst == 'X';
-  if (nh) return th ? k_cycle<true, true> : k_cycle<true, false>;
-  return th ? k_cycle<false, true> : k_cycle<false, false>;
+  if (S->P.precision == CLMD_PREC_MIXED) return cycle_kernel_mixed(nh, th);
+  if (nh) return th ? k_cycle<true, true, false> : k_cycle<true, false, false>;
+  return th ? k_cycle<false, true, false> : k_cycle<false, false, false>;
 }
 
 int cycle_blocks_for(clmd_system* S) {
@@ -1111,5 +1124,6 @@ void cycle_launch(clmd_system* S, int nsteps, int mode) {
   cudaLaunchKernelEx(&cfg, cycle_kernel(S), S->P, S->st, cycle_args(S), nsteps, mode);
   S->launches++;
 }
+#endif  // CLMD_CYCLE_MIXED
 
 }  // namespace clmd
