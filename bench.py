@@ -627,6 +627,51 @@ def batched_config_json(args, total, tuned, ngpu):
             "parallelism": f"replicas x{ngpu}"}
 
 
+def precision_check(specs, nsample=64, windows=20):
+    """The same replicas run twice, mixed and all-FP64 ensembles, for
+    windows x 100 Nose-Hoover steps: the relative drift of each replica's
+    conserved H = ekin + epot + Q PSI^2 / 2 + 3 N kT s (per 1e4 steps; the
+    reference's unshifted cut-off makes H drift in FP64 too) and the
+    cluster-size distribution at the end (sizes of every cluster of every
+    replica, Stillinger 1.5 sigma) compared as a total variation distance."""
+    sample = specs[:nsample]
+    out = {}
+    for prec, name in ((clmd.PREC_MIXED, "mixed"), (clmd.PREC_FP64, "fp64")):
+        e = clmd.Ensemble(clmd.ens_config(sum(n for n, _, _, _ in sample) + 64, len(sample),
+                                          precision=prec, integrator=clmd.INT_NOSE,
+                                          ftcsi=ENSEMBLE["ftcsi"], threads=256))
+        slots = {}
+        for n, rho, temp, sd in sample:
+            box = (n / rho) ** (1.0 / 3.0)
+            x, y, z, vx, vy, vz = clmd.init_random(n, (box, box, box), 0.9, temp, sd)
+            slots[e.add(n, box, temp, x, y, z, vx, vy, vz, csover=10**6, budget=0)] = (n, temp)
+
+        def H(r, n, temp):
+            return r.ekin + r.epot + 0.5 * (n * temp * 0.25) * r.psi ** 2 + 3.0 * n * temp * r.s
+
+        e.step(1)  # the start sequence and a first window: energies defined
+        h0 = {k: H(r, *slots[k]) for k, r in e.results().items()}
+        e.step(windows)
+        res = e.results()
+        drift = [abs(H(res[k], *slots[k]) - h0[k]) / abs(h0[k]) * 1e4 / (windows * 100)
+                 for k in slots]
+        sizes = []
+        for k in slots:
+            _, cl = e.state(k)
+            sizes.extend(np.bincount(cl)[1:][np.bincount(cl)[1:] > 0].tolist())
+        out[name] = (float(np.median(drift)), np.bincount(sizes))
+        e.close()
+    a, b = out["mixed"][1], out["fp64"][1]
+    m = max(len(a), len(b))
+    pa = np.pad(a, (0, m - len(a))).astype(float)
+    pb = np.pad(b, (0, m - len(b))).astype(float)
+    tv = 0.5 * np.abs(pa / pa.sum() - pb / pb.sum()).sum()
+    return {"replicas": nsample, "steps": windows * 100,
+            "energy_drift_per_1e4_steps_median": {"mixed": out["mixed"][0],
+                                                   "fp64": out["fp64"][0]},
+            "cluster_size_distribution_tv_distance": float(tv)}
+
+
 def mixed_force_error(e, slots, specs_by_slot, nsample=3):
     """Relative force error of the mixed engine against the FP64 oracle on
     the engine's own positions (normwise and worst atom above 1% of max)."""
@@ -737,6 +782,7 @@ def batched_arm(args):
     line = None
     if rank == 0:
         ferr_n, ferr_a = mixed_force_error(e, slots, slots)
+        pcheck = precision_check(specs)
         order = sorted(slots, key=lambda k: slots[k][0])
         picks = [order[int(q * (len(order) - 1))] for q in np.linspace(0, 1, args.dropin_sample)]
         rates = [(slots[k][0], dropin_rate(*slots[k])) for k in picks]
@@ -772,6 +818,7 @@ def batched_arm(args):
             "speedup_vs_fp64_dropin": value / dropin_value,
             "dropin_sample_rates": [[n, r] for n, r in rates],
             "force_rel_err_vs_fp64": {"normwise": ferr_n, "worst_atom": ferr_a},
+            "mixed_vs_fp64_sample": pcheck,
             "nucleated": sum(1 for r in res.values() if r.done == 1),
         }
         print(json.dumps(line), flush=True)
