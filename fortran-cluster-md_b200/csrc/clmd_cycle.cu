@@ -495,56 +495,12 @@ static __device__ bool rebuild(const Params& P, DevState* st, Blk& B, const Cycl
 }
 
 // for-a-lj-n-pbc-m.f:92-142 for one atom: fsum in the reference's order
+// (accumulated by warp_forces below)
 struct Pair {
   double fx, fy, fz, esum, vir;
 };
 
-__device__ __forceinline__ Pair pair_forces(const Params& P, DevState* st, const double4* pos,
-                                            const int* list, int k0, int k1, int kown,
-                                            const double4& pa, double bf1, double bf2) {
-  Pair r = {0.0, 0.0, 0.0, 0.0, 0.0};
-  int sa = (int)pa.w;
-  for (int k = k0; k < k1; k++) {
-    int j = list[k];
-    double4 pb = pos[j];
-    bool own = k >= kown;
-    double dx, dy, dz;
-    if (own) {
-      dx = pa.x - pb.x; dy = pa.y - pb.y; dz = pa.z - pb.z;
-    } else {
-      dx = pb.x - pa.x; dy = pb.y - pa.y; dz = pb.z - pa.z;
-    }
-    dx = mimage_bf(dx, P.boxx, P.ibx, bf1, bf2);
-    dy = mimage_bf(dy, P.boxy, P.iby, bf1, bf2);
-    dz = mimage_bf(dz, P.boxz, P.ibz, bf1, bf2);
-    double rij2 = dx * dx + dy * dy + dz * dz;
-    if (rij2 <= P.atr2) {
-      double r2 = rij2;
-      rij2 = 1.0 / rij2;
-      double rij6 = rij2 * rij2 * rij2;
-      int ij = sa + (int)pb.w;
-      if (ij < 2 || ij > 4) {
-        raise_err(st, CLMD_ERR_BAD_SPECIES);
-        continue;
-      }
-      double fij = pair_fij(P, ij, rij2, rij6);
-      if (own) {
-        r.esum = r.esum + pair_e(P, ij, rij6);
-        r.vir = r.vir + fij * r2;
-        r.fx = r.fx + fij * dx;
-        r.fy = r.fy + fij * dy;
-        r.fz = r.fz + fij * dz;
-      } else {
-        r.fx = r.fx - fij * dx;
-        r.fy = r.fy - fij * dy;
-        r.fz = r.fz - fij * dz;
-      }
-    }
-  }
-  return r;
-}
-
-// Warp-cooperative version for the 32 consecutive slots of a warp, whose
+// Pair forces, warp-cooperative, for the 32 consecutive slots of a warp, whose
 // rows are contiguous in the list (the search allocates them with one
 // warp-wide cursor step).  Lanes evaluate the pair terms of 32 consecutive
 // list entries at a time (balanced work whatever the row lengths), stage them
