@@ -344,3 +344,39 @@ def test_graph_replay_same_as_direct_launches(gpu, monkeypatch):
         for k in ("x", "vx", "az"):
             assert np.array_equal(getattr(xa, k), getattr(xb, k)), k
     assert a.results()[sa[3]].done == 2
+
+
+def test_failed_replica_is_isolated(gpu):
+    """A replica that fails (two atoms started 0.3 sigma apart: the skin is
+    exceeded in the first steps, neighbor-pbc-mav.f:48-51) stops with its own
+    status; the replicas beside it run on bit-identically to a batch without
+    it, and the batch keeps stepping."""
+    good = [(1500, 0.03, 81), (900, 0.04, 82), (3000, 0.02, 83)]
+
+    def build(with_bad):
+        e = clmd.Ensemble(clmd.ens_config(8000, 8, ftcsi=20, threads=256))
+        slots = []
+        for n, rho, sd in good:
+            box, arrs = replica_inputs(n, rho, 0.7, sd)
+            slots.append(e.add(n, box, 0.7, *arrs, csover=10**6, budget=400))
+        bad = None
+        if with_bad:
+            box, arrs = replica_inputs(1000, 0.03, 0.7, 84)
+            x, y, z = arrs[0].copy(), arrs[1].copy(), arrs[2].copy()
+            x[1], y[1], z[1] = x[0] + 0.3, y[0], z[0]
+            bad = e.add(1000, box, 0.7, x, y, z, *arrs[3:], csover=10**6, budget=400)
+        return e, slots, bad
+
+    a, sa, bad = build(True)
+    b, sb, _ = build(False)
+    for e in (a, b):
+        for _ in range(20):
+            e.step(1)
+    ra = a.results()
+    assert ra[bad].status != 0 and ra[bad].step < 400
+    for p, q in zip(sa, sb):
+        x, y = ra[p], b.results()[q]
+        assert x.status == 0 and (x.step, x.done, x.psi) == (y.step, y.done, y.psi)
+        xa, _ = a.state(p)
+        xb, _ = b.state(q)
+        assert np.array_equal(xa.x, xb.x) and np.array_equal(xa.vz, xb.vz)
