@@ -429,8 +429,13 @@ __device__ void forces(Rep& R, Cta& C, const Args& A, const Pos<SM>& P, bool kic
     double ax, ay, az;
     if (MIXED) {
       float fx = 0.f, fy = 0.f, fz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+      // the next row entry is loaded while this pair is evaluated
+      const int* lp = A.list + lbase + i;
+      int jn = len > 0 ? lp[0] : 0;
       for (int k = 0; k < len; k++) {
-        int j = A.list[lbase + (long long)k * N + i];
+        const int j = jn;
+        lp += N;
+        if (k + 1 < len) jn = *lp;
         double dx = mi_sel(xi - P.x(j), L, hL);
         double dy = mi_sel(yi - P.y(j), L, hL);
         double dz = mi_sel(zi - P.z(j), L, hL);
@@ -458,8 +463,13 @@ __device__ void forces(Rep& R, Cta& C, const Args& A, const Pos<SM>& P, bool kic
       az = (double)fz;
     } else {
       double fx = 0.0, fy = 0.0, fz = 0.0;
+      // the next row entry is loaded while this pair is evaluated
+      const int* lp = A.list + lbase + i;
+      int jn = len > 0 ? lp[0] : 0;
       for (int k = 0; k < len; k++) {
-        int j = A.list[lbase + (long long)k * N + i];
+        const int j = jn;
+        lp += N;
+        if (k + 1 < len) jn = *lp;
         double dx = mi_sel(xi - P.x(j), L, hL);
         double dy = mi_sel(yi - P.y(j), L, hL);
         double dz = mi_sel(zi - P.z(j), L, hL);
