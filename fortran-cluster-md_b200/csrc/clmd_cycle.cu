@@ -534,9 +534,16 @@ __device__ __forceinline__ void warp_forces(const Params& P, DevState* st, const
   fx = 0.0;
   fy = 0.0;
   fz = 0.0;
+  // this chunk's entry and neighbour position are fetched first, and the
+  // next chunk's entry with them, so that the loads overlap the owner search
+  int jnext = lane < tot ? list[wbase + lane] : 0;
   for (int c = 0; c < tot; c += 32) {
     const int k = c + lane;
     const int kk = k < tot ? k : tot - 1;
+    const int jc = jnext;
+    double4 pb = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (k < tot) pb = pos[jc];
+    if (k + 32 < tot) jnext = list[wbase + k + 32];
     int ow = 0;
 #pragma unroll
     for (int sft = 16; sft >= 1; sft >>= 1) {
@@ -553,8 +560,6 @@ __device__ __forceinline__ void warp_forces(const Params& P, DevState* st, const
     int flag = 0;
     double tx = 0.0, ty = 0.0, tz = 0.0;
     if (k < tot) {
-      int j = list[wbase + k];
-      double4 pb = pos[j];
       bool own = (k - oe) >= olo;  // neighbour has the larger reference index
       double dx, dy, dz;
       if (own) {
