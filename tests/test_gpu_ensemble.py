@@ -1,6 +1,6 @@
 """Ensembles (batched / served replicas) on the GPU against the FP64 oracle.
 
-Bars (north_star): mixed precision relative force error <= 1e-5 against the
+Bars: mixed precision relative force error <= 1e-5 against the
 FP64 oracle on the same positions; FP64 ensemble forces within 1e-12;
 cluster labels bit-exact on identical positions; a replica's result is the
 same alone and in a mix (bit-identical: per-replica work never depends on the

@@ -1,4 +1,4 @@
-"""Restart files and analysis writers (SURVEY's restart IO row): the
+"""Restart files and analysis writers: the
 reference's wrt-rst.f record layout, a restart that continues bit-identically,
 and the wrt-csi.f / wrt-csi-fre.f / wrt-fpt.f text formats checked against an
 independent Python restatement of their Fortran edit descriptors."""
