@@ -218,7 +218,8 @@ int clmd_init_random(int32_t n, double boxx, double boxy, double boxz, double rm
                      double* vx, double* vy, double* vz);
 
 /* ---------------------------------------------------------------------------
- * Ensembles: many independent replicas (configs "batched" and "served") in
+ * Ensembles: many independent replicas (batched nucleation runs, served
+ * requests) in
  * one persistent launch.  Reduced LJ units (sigma = eps = m = 1, one
  * species), the same per-replica algorithm as the drop-in (adaptive-skin
  * Verlet list, velocity Verlet or Nose-Hoover, Stillinger analysis every
