@@ -219,8 +219,7 @@ int clmd_init_random(int32_t n, double boxx, double boxy, double boxz, double rm
 
 /* ---------------------------------------------------------------------------
  * Ensembles: many independent replicas (batched nucleation runs, served
- * requests) in
- * one persistent launch.  Reduced LJ units (sigma = eps = m = 1, one
+ * requests) in one persistent launch.  Reduced LJ units (sigma = eps = m = 1, one
  * species), the same per-replica algorithm as the drop-in (adaptive-skin
  * Verlet list, velocity Verlet or Nose-Hoover, Stillinger analysis every
  * ftcsi steps, chk_nucleation), with FP32 pair terms accumulated per atom in
