@@ -606,24 +606,47 @@ __device__ __forceinline__ void warp_forces(const Params& P, DevState* st, const
         }
       }
     }
+    const int a0 = e > c ? e : c;
+    const int a1 = (e + len) < (c + 32) ? (e + len) : (c + 32);
+    if (mixed) {
+      // each row's terms in this chunk summed by a segmented scan across the
+      // lanes (a fixed tree: deterministic), then added to the owner's
+      // Kahan sums chunk by chunk: every lane works, where the ordered
+      // FP64 sum below has only the owners working
+      const float sg = flag == 1 ? 1.0f : (flag == 2 ? -1.0f : 0.0f);
+      float v0 = sg * (float)tx, v1 = sg * (float)ty, v2 = sg * (float)tz;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const int ou = __shfl_up_sync(FULL, ow, off);
+        const float u0 = __shfl_up_sync(FULL, v0, off);
+        const float u1 = __shfl_up_sync(FULL, v1, off);
+        const float u2 = __shfl_up_sync(FULL, v2, off);
+        if (lane >= off && ou == ow) {
+          v0 = __fadd_rn(v0, u0);
+          v1 = __fadd_rn(v1, u1);
+          v2 = __fadd_rn(v2, u2);
+        }
+      }
+      const int last = a1 > a0 ? a1 - 1 - c : 0;  // my row's last entry in the chunk
+      const float p0 = __shfl_sync(FULL, v0, last);
+      const float p1 = __shfl_sync(FULL, v1, last);
+      const float p2 = __shfl_sync(FULL, v2, last);
+      if (a1 > a0) {
+        kahan_add(sx, kx, p0);
+        kahan_add(sy, ky, p1);
+        kahan_add(sz, kz, p2);
+      }
+      continue;
+    }
     W.tx[lane] = tx;
     W.ty[lane] = ty;
     W.tz[lane] = tz;
     W.flag[lane] = flag;
     __syncwarp();
-    const int a0 = e > c ? e : c;
-    const int a1 = (e + len) < (c + 32) ? (e + len) : (c + 32);
     for (int a = a0; a < a1; a++) {
       int q = a - c;
       int f = W.flag[q];
-      if (mixed) {
-        if (f) {
-          const float sg = f == 1 ? 1.0f : -1.0f;
-          kahan_add(sx, kx, sg * (float)W.tx[q]);
-          kahan_add(sy, ky, sg * (float)W.ty[q]);
-          kahan_add(sz, kz, sg * (float)W.tz[q]);
-        }
-      } else if (f == 1) {
+      if (f == 1) {
         fx = fx + W.tx[q];
         fy = fy + W.ty[q];
         fz = fz + W.tz[q];
