@@ -506,9 +506,13 @@ struct Pair {
 // list entries at a time (balanced work whatever the row lengths), stage them
 // in shared memory, and each owner lane then adds its own terms in list
 // order, i.e. in the reference's order, with the same +/- as the serial code.
+// FP64: the terms of kGroup chunks are staged before the owner lanes add
+// theirs, so that more owners work at once (a row's terms still go in
+// list order)
+constexpr int kGroup = 4;
 struct WarpStage {
-  double tx[32], ty[32], tz[32];
-  int flag[32];  // 0 nothing, 1 add, 2 subtract
+  double tx[32 * kGroup], ty[32 * kGroup], tz[32 * kGroup];
+  int flag[32 * kGroup];  // 0 nothing, 1 add, 2 subtract
 };
 
 template <bool MIXED>
@@ -638,13 +642,18 @@ __device__ __forceinline__ void warp_forces(const Params& P, DevState* st, const
       }
       continue;
     }
-    W.tx[lane] = tx;
-    W.ty[lane] = ty;
-    W.tz[lane] = tz;
-    W.flag[lane] = flag;
+    const int g = (c >> 5) % kGroup;
+    W.tx[32 * g + lane] = tx;
+    W.ty[32 * g + lane] = ty;
+    W.tz[32 * g + lane] = tz;
+    W.flag[32 * g + lane] = flag;
+    if (g != kGroup - 1 && c + 32 < tot) continue;  // the group is not full yet
     __syncwarp();
-    for (int a = a0; a < a1; a++) {
-      int q = a - c;
+    const int cg = c - 32 * g;  // the group's first entry
+    const int b0 = e > cg ? e : cg;
+    const int b1 = (e + len) < (c + 32) ? (e + len) : (c + 32);
+    for (int a = b0; a < b1; a++) {
+      int q = a - cg;
       int f = W.flag[q];
       if (f == 1) {
         fx = fx + W.tx[q];
