@@ -509,7 +509,10 @@ struct Pair {
 // FP64: the terms of kGroup chunks are staged before the owner lanes add
 // theirs, so that more owners work at once (a row's terms still go in
 // list order)
-constexpr int kGroup = 4;
+#ifndef CLMD_FORCE_GROUP
+#define CLMD_FORCE_GROUP 4
+#endif
+constexpr int kGroup = CLMD_FORCE_GROUP;
 struct WarpStage {
   double tx[32 * kGroup], ty[32 * kGroup], tz[32 * kGroup];
   int flag[32 * kGroup];  // 0 nothing, 1 add, 2 subtract
