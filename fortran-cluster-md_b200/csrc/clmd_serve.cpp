@@ -22,7 +22,8 @@ struct Prepared {
   int status = -1;  // -1 pending, CLMD_OK ready, else the generator's error
 };
 
-// host worker pool: start states in arrival order, ahead of admission
+// host worker pool: start states in arrival order, at most kAhead requests
+// ahead of admission (a long trace's states are not all held in memory)
 class Generator {
  public:
   Generator(const clmd_request* reqs, int n, int threads) : reqs_(reqs), n_(n), prep_(n) {
@@ -37,6 +38,8 @@ class Generator {
     return prep_[k].status != -1;
   }
   Prepared& get(int k) { return prep_[k]; }
+  // requests before k have been admitted or dropped
+  void consumed(int k) { consumed_ = k; }
   void release(int k) {
     std::lock_guard<std::mutex> lock(mu_);
     Prepared& p = prep_[k];
@@ -54,6 +57,10 @@ class Generator {
       if (stop_) return;
       int k = next_.fetch_add(1);
       if (k >= n_) return;
+      while (k >= consumed_.load() + kAhead) {
+        if (stop_) return;
+        std::this_thread::sleep_for(std::chrono::microseconds(500));
+      }
       const clmd_request& r = reqs_[k];
       Prepared p;
       const int n = r.natom;
@@ -72,7 +79,9 @@ class Generator {
   int n_;
   std::vector<Prepared> prep_;
   std::vector<std::thread> pool_;
+  static constexpr int kAhead = 256;
   std::atomic<int> next_{0};
+  std::atomic<int> consumed_{0};
   std::atomic<bool> stop_{false};
   std::mutex mu_;
 };
@@ -127,6 +136,7 @@ extern "C" int clmd_serve(clmd_ensemble* e, const clmd_request* reqs, int32_t nr
         out[next].status = p.status;
         gen.release(next);
         next++;
+        gen.consumed(next);
         continue;
       }
       clmd_replica_spec sp;
@@ -155,6 +165,7 @@ extern "C" int clmd_serve(clmd_ensemble* e, const clmd_request* reqs, int32_t nr
       resident_atoms += sp.natom;
       S.admitted++;
       next++;
+      gen.consumed(next);
     }
     if (st) break;
     if (resident > S.peak_resident) S.peak_resident = resident;
