@@ -981,7 +981,7 @@ struct clmd_ensemble {
   bool reps_stale = false;    // h_reps older than the device records
   // size classes: each has its own block size, shared-memory budget, stream
   static constexpr int kClasses = 4;
-  int cls_max[kClasses] = {1024, 2560, 6144, 1 << 30};
+  int cls_max[kClasses] = {1536, 3072, 6144, 1 << 30};  // measured best of a few splits
   int cls_threads[kClasses] = {128, 256, 512, 1024};
   cudaStream_t cstream[kClasses] = {};
   cudaEvent_t ev0[kClasses] = {}, ev1[kClasses] = {}, evj = nullptr;
@@ -1064,6 +1064,13 @@ extern "C" int clmd_ens_create(const clmd_ens_config* cfg, clmd_ensemble** out) 
   {
     const char* g = getenv("CLMD_ENS_GRAPHS");
     E->use_graphs = !(g && g[0] == '0');
+    // CLMD_ENS_CLASSES="a,b,c": upper atom counts of the first three size
+    // classes (ascending), for tuning the split
+    const char* cs = getenv("CLMD_ENS_CLASSES");
+    int b[3];
+    if (cs && sscanf(cs, "%d,%d,%d", &b[0], &b[1], &b[2]) == 3 && 0 < b[0] && b[0] < b[1] &&
+        b[1] < b[2])
+      for (int c = 0; c < 3; c++) E->cls_max[c] = b[c];
   }
   E->tuned = cfg->threads > 0;
   const long long P = cfg->max_atoms;

@@ -287,7 +287,7 @@ int clmd_ens_step(clmd_ensemble* e, int32_t nwin);
  * and trajectories are those of clmd_ens_step. */
 int clmd_ens_step_timed(clmd_ensemble* e, float ms);
 /* Autotuner: picks the block size of each of the 4 replica-size classes
- * (atoms <= 1024, <= 2560, <= 6144, larger) from {128, 256, 512, 1024} by
+ * (atoms <= 1536, <= 3072, <= 6144, larger) from {128, 256, 512, 1024} by
  * timing one window per candidate on the running replicas; those 4 windows
  * advance the simulation.  threads_out (4 entries, may be NULL) gets the
  * choice.  Without it the classes use 128/256/512/1024 threads, or
