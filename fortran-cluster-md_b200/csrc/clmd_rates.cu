@@ -117,6 +117,11 @@ __global__ void k_gas_ekin(int n, const double* cek, const unsigned long long* k
 // scalev-clu.f:58-59: kfG and kfC from the block sums, added in order
 __global__ void k_clu_factors(Params P, int nb, const double* partials, const int* cs,
                               const double* cek, const unsigned long long* key, double* kf) {
+  if (*key == 0) {  // no cluster record (no analysis has run): leave v alone
+    kf[0] = 1.0;
+    kf[1] = 1.0;
+    return;
+  }
   double ekinG = 0.0;
   for (int b = 0; b < nb; b++) ekinG += partials[b];
   const int ci = key_label(*key) - 1;
