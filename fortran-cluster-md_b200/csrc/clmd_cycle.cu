@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 #include <stdio.h>
 
+#include "clmd_nh.cuh"
 #include "clmd_system.hpp"
 
 namespace clmd {
@@ -888,6 +889,14 @@ __global__ void __launch_bounds__(kPB, CLMD_CYCLE_MINB) k_cycle(Params P, DevSta
             A.vx[p] = vxi;
             A.vy[p] = vyi;
             A.vz[p] = vzi;
+          } else if (MIXED) {
+            // closed-form solve (clmd_nh_root): W = V + dth a in place of V,
+            // sv = sum W^2
+            double wx = A.vx[p] + dth * axi, wy = A.vy[p] + dth * ayi, wz = A.vz[p] + dth * azi;
+            A.vx[p] = wx;
+            A.vy[p] = wy;
+            A.vz[p] = wz;
+            sv = sv + wx * wx + wy * wy + wz * wz;
           } else {
             // int-verlet-nh-mav.f:94-120: vn = V, sumv2, first sweep's delps
             double vxi = A.vx[p], vyi = A.vy[p], vzi = A.vz[p];
@@ -952,6 +961,33 @@ __global__ void __launch_bounds__(kPB, CLMD_CYCLE_MINB) k_cycle(Params P, DevSta
         double sumv2 = get_sum(red(), SLOT_SUMV2, sh, B.bcast);
         double draw = get_sum(red(), SLOT_DELPS, sh, B.bcast);
         rb ^= 1;
+        if (MIXED) {
+          // every block solves the same scalar equation from the same sums
+          double pn;
+          if (!clmd_nh_root(m * sumv2, psi, P.nkt3_i, dth, Q, pn)) {
+            if (threadIdx.x == 0 && B.q.status == 0) {
+              B.q.status = CLMD_ERR_NH_NOCONVERGE;
+              B.q.fail_step = step;
+            }
+            __syncthreads();
+            goto done;
+          }
+          const double c = 1.0 / (1.0 + dth * pn);
+          for (int p = t0; p < N; p += G) {
+            A.vx[p] = A.vx[p] * c;
+            A.vy[p] = A.vy[p] * c;
+            A.vz[p] = A.vz[p] * c;
+          }
+          if (threadIdx.x == 0) {
+            B.q.nh_iters = 1;
+            B.q.sumv2 = sumv2 * c * c;
+            B.q.psi = pn;
+            B.q.ekin = 0.5 * m * B.q.sumv2;
+          }
+          __syncthreads();
+          drift_done = false;
+          continue;
+        }
         double psn = psi;
         int ready = 0, iter;
         for (iter = 1; iter <= 1000; iter++) {

@@ -32,6 +32,7 @@
 #include <vector>
 
 #include "../../include/clmd.h"
+#include "clmd_nh.cuh"
 
 namespace clmd_ens {
 
@@ -495,7 +496,17 @@ __device__ void forces(Rep& R, Cta& C, const Args& A, const Pos<SM>& P, bool kic
       ay = fy;
       az = fz;
     }
-    if (NHF) {
+    if (NHF && MIXED) {
+      // closed-form solve (clmd_nh_root): W = V + dth a into vn, s0 += W.W
+      const double dth = 0.5 * dt;
+      const double wx = A.vx[off + i] + dth * ax;
+      const double wy = A.vy[off + i] + dth * ay;
+      const double wz = A.vz[off + i] + dth * az;
+      A.vxn[off + i] = wx;
+      A.vyn[off + i] = wy;
+      A.vzn[off + i] = wz;
+      *s0 += wx * wx + wy * wy + wz * wz;
+    } else if (NHF) {
       const double dth = 0.5 * dt;
       const double V[3] = {A.vx[off + i], A.vy[off + i], A.vz[off + i]};
       const double a3[3] = {ax, ay, az};
@@ -672,6 +683,7 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
   const double dt = A.dt;
   Pos<SM> P{A, C, off};
   bool vin_n = false;  // uniform: the current velocities are in vxn, not vx
+  double vsc = 1.0;    // mixed: the velocities are vn * vsc (clmd_nh_root)
   if (SM) {
     for (int i = tid; i < N; i += NT) {
       C.sx[i] = A.x[off + i];
@@ -718,9 +730,9 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
     if (A.ftcsi > 0 && R.step % A.ftcsi == 0 && R.cstep != R.step) {
       if (vin_n) {  // velocities back in vx for the analysis
         for (int i = tid; i < N; i += NT) {
-          A.vx[off + i] = A.vxn[off + i];
-          A.vy[off + i] = A.vyn[off + i];
-          A.vz[off + i] = A.vzn[off + i];
+          A.vx[off + i] = MIXED ? A.vxn[off + i] * vsc : A.vxn[off + i];
+          A.vy[off + i] = MIXED ? A.vyn[off + i] * vsc : A.vyn[off + i];
+          A.vz[off + i] = MIXED ? A.vzn[off + i] * vsc : A.vzn[off + i];
         }
         vin_n = false;
         __syncthreads();
@@ -744,9 +756,15 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
       const double* svx = vin_n ? A.vxn : A.vx;
       const double* svy = vin_n ? A.vyn : A.vy;
       const double* svz = vin_n ? A.vzn : A.vz;
+      const double sc = vin_n ? vsc : 1.0;
       vin_n = false;
       for (int i = tid; i < N; i += NT) {
         double vxi = svx[off + i], vyi = svy[off + i], vzi = svz[off + i];
+        if (MIXED) {
+          vxi = vxi * sc;
+          vyi = vyi * sc;
+          vzi = vzi * sc;
+        }
         double axi, ayi, azi;
         get_a<MIXED>(A, off + i, axi, ayi, azi);
         double dx, dy, dz;
@@ -797,63 +815,82 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
         // next sweep's sums (sum vn^2, sum b vo dt/Q at pso + delps) in the
         // same loop; the first pass rides on the force pass.
         const double Q = R.Q, err = 1.0e-10, psi1 = R.psi, dtQ = dt / Q;
-        double sumv2n = 0.0, dpsum = 0.0;
-        forces<NT, SM, MIXED, true>(R, C, A, P, false, last, psi1, dtQ, &sumv2n, &dpsum);
-        int nr0 = 0;
-        cta_sum2<NT>(sumv2n, dpsum, nr0, C.red);
-        double psn = psi1;
-        int ready = 0;
-        for (int iter = 1; iter <= 1000; iter++) {
-          const double pso = psn;
-          const double di = -(pso * dth + 1);
-          double delps = dpsum - di * ((-sumv2n + R.nkt3_i) * dth / Q - (psi1 - pso));
-          delps = delps / (-dt2 * sumv2n / Q + di);
-          psn = pso + delps;
-          const double rdi = 1.0 / di;
-          double s2 = 0.0, dpn = 0.0;
-          int nr = 0;
-          for (int i = tid; i < N; i += NT) {
-            double ax, ay, az;
-            get_a<MIXED>(A, off + i, ax, ay, az);
-            const double V[3] = {A.vx[off + i], A.vy[off + i], A.vz[off + i]};
-            const double a3[3] = {ax, ay, az};
-            double* vn[3] = {A.vxn, A.vyn, A.vzn};
-            // the update rounded term by term: with fused multiply-adds the
-            // residual b never reaches exactly zero, the sweep keeps moving a
-            // near-zero component by ~1e-18 and the relative test then fails
-            // where the reference's sweep (int-verlet-nh-mav.f:117-147)
-            // settles on an exact fixed point
-#pragma unroll
-            for (int d = 0; d < 3; d++) {
-              const double vo = vn[d][off + i];
-              const double b = __dsub_rn(__dmul_rn(-dth, __dsub_rn(a3[d], __dmul_rn(pso, vo))),
-                                         __dsub_rn(V[d], vo));
-              const double nx =
-                  __dadd_rn(vo, __dmul_rn(__dadd_rn(b, __dmul_rn(__dmul_rn(dth, vo), delps)), rdi));
-              if (fabs(__dsub_rn(nx, vo)) > err * fabs(nx)) nr = 1;
-              vn[d][off + i] = nx;
-              s2 += nx * nx;
-              dpn += (-dth * (a3[d] - psn * nx) - (V[d] - nx)) * nx * dtQ;
+        if (MIXED) {
+          double S = 0.0, unused = 0.0, p;
+          int nr0 = 0;
+          forces<NT, SM, MIXED, true>(R, C, A, P, false, last, psi1, dtQ, &S, &unused);
+          cta_sum2<NT>(S, unused, nr0, C.red);
+          if (!clmd_nh_root(S, psi1, R.nkt3_i, dth, Q, p)) {
+            if (tid == 0 && R.status == 0) R.status = CLMD_ERR_NH_NOCONVERGE;
+            __syncthreads();
+            goto out;
+          }
+          vsc = 1.0 / (1.0 + dth * p);
+          vin_n = true;
+          if (tid == 0) {
+            R.sumv2 = S * vsc * vsc;
+            R.psi = p;
+            R.ekin = 0.5 * R.sumv2;
+          }
+        } else {
+          double sumv2n = 0.0, dpsum = 0.0;
+          forces<NT, SM, MIXED, true>(R, C, A, P, false, last, psi1, dtQ, &sumv2n, &dpsum);
+          int nr0 = 0;
+          cta_sum2<NT>(sumv2n, dpsum, nr0, C.red);
+          double psn = psi1;
+          int ready = 0;
+          for (int iter = 1; iter <= 1000; iter++) {
+            const double pso = psn;
+            const double di = -(pso * dth + 1);
+            double delps = dpsum - di * ((-sumv2n + R.nkt3_i) * dth / Q - (psi1 - pso));
+            delps = delps / (-dt2 * sumv2n / Q + di);
+            psn = pso + delps;
+            const double rdi = 1.0 / di;
+            double s2 = 0.0, dpn = 0.0;
+            int nr = 0;
+            for (int i = tid; i < N; i += NT) {
+              double ax, ay, az;
+              get_a<MIXED>(A, off + i, ax, ay, az);
+              const double V[3] = {A.vx[off + i], A.vy[off + i], A.vz[off + i]};
+              const double a3[3] = {ax, ay, az};
+              double* vn[3] = {A.vxn, A.vyn, A.vzn};
+              // the update rounded term by term: with fused multiply-adds the
+              // residual b never reaches exactly zero, the sweep keeps moving a
+              // near-zero component by ~1e-18 and the relative test then fails
+              // where the reference's sweep (int-verlet-nh-mav.f:117-147)
+              // settles on an exact fixed point
+  #pragma unroll
+              for (int d = 0; d < 3; d++) {
+                const double vo = vn[d][off + i];
+                const double b = __dsub_rn(__dmul_rn(-dth, __dsub_rn(a3[d], __dmul_rn(pso, vo))),
+                                           __dsub_rn(V[d], vo));
+                const double nx =
+                    __dadd_rn(vo, __dmul_rn(__dadd_rn(b, __dmul_rn(__dmul_rn(dth, vo), delps)), rdi));
+                if (fabs(__dsub_rn(nx, vo)) > err * fabs(nx)) nr = 1;
+                vn[d][off + i] = nx;
+                s2 += nx * nx;
+                dpn += (-dth * (a3[d] - psn * nx) - (V[d] - nx)) * nx * dtQ;
+              }
+            }
+            sumv2n = s2;
+            dpsum = dpn;
+            cta_sum2<NT>(sumv2n, dpsum, nr, C.red);
+            if (!nr) {
+              ready = 1;
+              break;
             }
           }
-          sumv2n = s2;
-          dpsum = dpn;
-          cta_sum2<NT>(sumv2n, dpsum, nr, C.red);
-          if (!nr) {
-            ready = 1;
-            break;
+          if (!ready) {
+            if (tid == 0 && R.status == 0) R.status = CLMD_ERR_NH_NOCONVERGE;
+            __syncthreads();
+            goto out;
           }
-        }
-        if (!ready) {
-          if (tid == 0 && R.status == 0) R.status = CLMD_ERR_NH_NOCONVERGE;
-          __syncthreads();
-          goto out;
-        }
-        vin_n = true;  // the step's velocities are in vxn until the next drift
-        if (tid == 0) {
-          R.sumv2 = sumv2n;
-          R.psi = psn;
-          R.ekin = 0.5 * sumv2n;
+          vin_n = true;  // the step's velocities are in vxn until the next drift
+          if (tid == 0) {
+            R.sumv2 = sumv2n;
+            R.psi = psn;
+            R.ekin = 0.5 * sumv2n;
+          }
         }
       }
       if (tid == 0) R.step = step + 1;
@@ -864,9 +901,9 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
     if (R.step >= R.budget) {
       if (vin_n) {
         for (int i = tid; i < N; i += NT) {
-          A.vx[off + i] = A.vxn[off + i];
-          A.vy[off + i] = A.vyn[off + i];
-          A.vz[off + i] = A.vzn[off + i];
+          A.vx[off + i] = MIXED ? A.vxn[off + i] * vsc : A.vxn[off + i];
+          A.vy[off + i] = MIXED ? A.vyn[off + i] * vsc : A.vyn[off + i];
+          A.vz[off + i] = MIXED ? A.vzn[off + i] * vsc : A.vzn[off + i];
         }
         vin_n = false;
         __syncthreads();
@@ -883,9 +920,9 @@ out:
   __syncthreads();
   if (vin_n) {
     for (int i = tid; i < N; i += NT) {
-      A.vx[off + i] = A.vxn[off + i];
-      A.vy[off + i] = A.vyn[off + i];
-      A.vz[off + i] = A.vzn[off + i];
+      A.vx[off + i] = MIXED ? A.vxn[off + i] * vsc : A.vxn[off + i];
+      A.vy[off + i] = MIXED ? A.vyn[off + i] * vsc : A.vyn[off + i];
+      A.vz[off + i] = MIXED ? A.vzn[off + i] * vsc : A.vzn[off + i];
     }
   }
   if (SM) {

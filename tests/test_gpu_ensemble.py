@@ -62,6 +62,36 @@ def test_ensemble_forces_against_oracle(gpu, precision, tol):
     assert all(r.status == 0 for r in res.values())
 
 
+def test_mixed_ensemble_nose_hoover_tracks_fp64(gpu):
+    """The mixed ensemble (FP32 pair terms, the implicit Nose-Hoover velocity
+    step solved in closed form) against the FP64 ensemble (the reference's
+    Newton sweeps, int-verlet-nh-mav.f:105-147) on the same replicas over one
+    50-step window: velocities and ekin within 1e-6 relative, PSI within 1e-6
+    of its scale 3NkT dt steps / Q (the FP32 pair terms set these gaps)."""
+    specs = [(1500, 0.05, 0.7), (800, 0.02, 0.8), (3000, 0.04, 0.75)]
+    out = {}
+    for prec in (clmd.PREC_MIXED, clmd.PREC_FP64):
+        e = clmd.Ensemble(clmd.ens_config(20000, 8, precision=prec, ftcsi=50))
+        slots = []
+        for k, (n, rho, temp) in enumerate(specs):
+            box, arrs = replica_inputs(n, rho, temp, 300 + k)
+            slots.append(e.add(n, box, temp, *arrs))
+        e.step(1)
+        res = e.results()
+        out[prec] = [(e.state(sl)[0], res[sl]) for sl in slots]
+    for (n, rho, temp), (a, ra), (b, rb) in zip(specs, out[clmd.PREC_MIXED],
+                                                out[clmd.PREC_FP64]):
+        assert ra.status == 0 and rb.status == 0 and ra.step == rb.step == 50
+        va = np.stack([a.vx, a.vy, a.vz])
+        vb = np.stack([b.vx, b.vy, b.vz])
+        dv = np.linalg.norm(va - vb) / np.linalg.norm(vb)
+        scale = 3.0 * n * temp * 0.005 * 50 / (n * temp * 0.25)
+        dpsi = abs(ra.psi - rb.psi) / scale
+        dek = abs(ra.ekin - rb.ekin) / rb.ekin
+        print(f"N={n}: dv {dv:.2e} dpsi {dpsi:.2e} dekin {dek:.2e}")
+        assert dv <= 1e-6 and dpsi <= 1e-6 and dek <= 1e-6, (n, dv, dpsi, dek)
+
+
 def test_ensemble_cluster_labels_exact(gpu):
     e = clmd.Ensemble(clmd.ens_config(10000, 4, ftcsi=20))
     n, rho = 4000, 0.3
@@ -221,14 +251,18 @@ def test_balanced_step_same_trajectories(gpu):
         assert np.array_equal(ca, cb)
 
 
-def test_nose_hoover_solve_converges_over_long_runs(gpu):
-    """1.5e9 atom-steps of Nose-Hoover without CLMD_ERR_NH_NOCONVERGE.  The
-    reference's per-component relative test (int-verlet-nh-mav.f:140-147)
+@pytest.mark.parametrize("precision", [clmd.PREC_MIXED, clmd.PREC_FP64])
+def test_nose_hoover_solve_converges_over_long_runs(gpu, precision):
+    """1.5e9 atom-steps of Nose-Hoover without CLMD_ERR_NH_NOCONVERGE.  FP64:
+    the reference's per-component relative test (int-verlet-nh-mav.f:140-147)
     passes because its sweep reaches an exact fixed point; a sweep evaluated
     with fused multiply-adds does not, and failed here about once per 4e8
-    atom-steps."""
+    atom-steps.  Mixed: the closed-form root's Newton steps must settle above
+    the rounding noise of f(p) (a limit at 1e-16 of the scale stalled on 3 of
+    these 128 replicas)."""
     rng = np.random.default_rng(12)
-    e = clmd.Ensemble(clmd.ens_config(128 * 4000, 128, ftcsi=100, threads=256))
+    e = clmd.Ensemble(clmd.ens_config(128 * 4000, 128, ftcsi=100, threads=256,
+                                      precision=precision))
     for k in range(128):
         rho, temp = float(rng.uniform(0.03, 0.05)), float(rng.uniform(0.65, 0.85))
         box, arrs = replica_inputs(4000, rho, temp, 9000 + k)

@@ -90,6 +90,53 @@ def nh_energy(g, cfg):
     return q.ekin + q.epot + 0.5 * cfg.Q * q.psi ** 2 + nkt3 * q.s
 
 
+def test_mixed_nose_hoover_step_against_oracle_sweeps(gpu):
+    """The mixed engine solves the implicit Nose-Hoover velocity step in
+    closed form (the fixed point of int-verlet-nh-mav.f:105-147); the oracle
+    runs the reference's Newton sweeps to their 1e-10 test.  From identical
+    injected states the positions agree exactly (the drift is FP64) and every
+    gap after the step is what the FP32 pair terms explain: with da the
+    accelerations' gap, v = (V + dth a) / (1 + dth PSI) moves by at most
+    dth |da| (x1.5), PSI by 2 dth^2 |v| |da| / Q (x2), ekin by |v| |dv|, on
+    top of 1e-10 (the sweeps' own test)."""
+    from conftest import start_pair
+    cfg = nvt_config(3000, clmd.PREC_MIXED)
+    dth = 0.5 * cfg.dt
+    st = random_state(cfg, 21)
+    g = clmd.System(cfg)
+    o = orc.Oracle(cfg)
+    start_pair(g, o, cfg, st)
+    s0 = o.scalars()
+    psi = (2.0 * s0.ekin - 3.0 * cfg.natom * clmd.CIKB * cfg.att) / cfg.Q
+    for sysx in (g, o):
+        s = sysx.scalars()
+        s.psi, s.s = psi, 0.0
+        sysx.set_scalars(s)
+    for step in range(1, 6):
+        ref, so = o.get_state(), o.scalars()
+        g.set_state(ref, scalars=so)
+        g.integrator(step)
+        o.integrator(step)
+        a, b = g.get_state(), o.get_state()
+        for k in ("x", "y", "z"):
+            assert np.array_equal(getattr(a, k), getattr(b, k)), k
+        aa = np.stack([a.ax, a.ay, a.az])
+        ab = np.stack([b.ax, b.ay, b.az])
+        da = np.linalg.norm(aa - ab)
+        assert da <= 1e-5 * np.linalg.norm(ab)
+        va = np.stack([a.vx, a.vy, a.vz])
+        vb = np.stack([b.vx, b.vy, b.vz])
+        nv = np.linalg.norm(vb)
+        dv = np.linalg.norm(va - vb)
+        assert dv <= 1.5 * dth * da + 1e-10 * nv, (dv, dth * da)
+        sg, so = g.scalars(), o.scalars()
+        assert sg.status == 0 and sg.nh_iters == 1 and so.nh_iters >= 2
+        dpsi = abs(sg.psi - so.psi)
+        assert dpsi <= 4.0 * dth * dth * nv * da / cfg.Q + 1e-10 * abs(so.psi), dpsi
+        assert abs(sg.ekin - so.ekin) <= nv * dv + 1e-10 * so.ekin
+    g.close()
+
+
 def test_mixed_energy_drift_tracks_fp64(gpu):
     """H = ekin + epot + Q PSI^2 / 2 + 3 N kT s over 1e4 Nose-Hoover steps.
     The truncated (unshifted) LJ of the reference loses energy whenever a pair
