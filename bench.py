@@ -626,7 +626,7 @@ def batched_config_json(args, total, tuned, ngpu):
             "replicas_per_gpu": args.replicas, "atoms_per_gpu": total,
             "steps_per_bench_step": 100, "clustering": "stillinger-1.5sigma every 100",
             "stop": "largest cluster > 50 (csover=51) or 2e5 steps",
-            "threads_per_size_class": tuned,
+            "threads_per_size_class": [clmd.shape_name(t) for t in tuned],
             "l2": "window state (~1 GB) larger than L2; no flush needed",
             "parallelism": f"replicas x{ngpu}"}
 

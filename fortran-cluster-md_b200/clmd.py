@@ -582,6 +582,15 @@ class System:
         return out
 
 
+ENS_LEAN = 0x10000  # CLMD_ENS_LEAN: the 64-register variant of a 128/256/512-thread CTA
+
+
+def shape_name(shape):
+    """A block shape as text: '256' or '256 lean (64 regs)'."""
+    t = shape & 0xFFFF
+    return f"{t} lean (64 regs)" if shape & ENS_LEAN else str(t)
+
+
 def ens_config(max_atoms, max_replicas, *, precision=PREC_MIXED, integrator=INT_NOSE, ftcsi=100,
                rc=2.5, rskin=2.8, atskin=1.5, dt=0.005, nbtim=10, list_stride=0, threads=0):
     c = EnsConfig()
@@ -647,7 +656,8 @@ class Ensemble:
             raise ClmdError(st, "clmd_ens_step_timed")
 
     def autotune(self):
-        """Block size per replica-size class, picked by timing (4 windows)."""
+        """Block shape per replica-size class, picked by timing (7 windows):
+        threads per CTA, | ENS_LEAN for the 64-register variant."""
         out = (C.c_int32 * 4)()
         st = self.lib.clmd_ens_autotune(self.h, out)
         if st:

@@ -935,8 +935,10 @@ out:
   __syncthreads();
 }
 
-template <int NT, bool SM, bool MIXED>
-__global__ void __launch_bounds__(NT, (NT < 512 ? 512 / NT : 1)) k_ens(Args A) {
+// MINB: CTAs per SM the register budget must allow -- 512 / NT (<= 128
+// registers per thread) or, for the register-lean shapes, 1024 / NT (64)
+template <int NT, bool SM, bool MIXED, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_ens(Args A) {
   extern __shared__ double dsm[];
   __shared__ Rep R;
   __shared__ Cta C;
@@ -1018,7 +1020,7 @@ struct clmd_ensemble {
   bool reps_stale = false;    // h_reps older than the device records
   // size classes: each has its own block size, shared-memory budget, stream
   static constexpr int kClasses = 4;
-  int cls_max[kClasses] = {1536, 3072, 6144, 1 << 30};  // measured best of a few splits
+  int cls_max[kClasses] = {2048, 4096, 6144, 1 << 30};  // measured best of a few splits
   int cls_threads[kClasses] = {128, 256, 512, 1024};
   cudaStream_t cstream[kClasses] = {};
   cudaEvent_t ev0[kClasses] = {}, ev1[kClasses] = {}, evj = nullptr;
@@ -1067,9 +1069,20 @@ static int cells_for(size_t cap, int nmax, bool* sm) {
   return kNcMax;
 }
 
+// the block shapes k_ens is compiled for (0: autotune)
+static bool shape_ok(int shape) {
+  switch (shape) {
+    case 0: case 128: case 256: case 512: case 1024:
+    case 128 | CLMD_ENS_LEAN: case 256 | CLMD_ENS_LEAN: case 512 | CLMD_ENS_LEAN:
+      return true;
+    default:
+      return false;
+  }
+}
+
 extern "C" int clmd_ens_create(const clmd_ens_config* cfg, clmd_ensemble** out) {
   if (!cfg || !out || cfg->max_atoms < 2 || cfg->max_replicas < 1 || cfg->dt <= 0 ||
-      cfg->rc <= 0 || cfg->rskin < cfg->rc || cfg->nbtim < 1)
+      cfg->rc <= 0 || cfg->rskin < cfg->rc || cfg->nbtim < 1 || !shape_ok(cfg->threads))
     return CLMD_ERR_ARG;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
@@ -1315,18 +1328,23 @@ extern "C" int clmd_ens_remove(clmd_ensemble* E, int32_t slot) {
 
 typedef void (*EnsKernel)(Args);
 
-template <int NT>
+template <int NT, int MINB>
 static EnsKernel pick(bool sm, bool mixed) {
-  if (sm) return mixed ? k_ens<NT, true, true> : k_ens<NT, true, false>;
-  return mixed ? k_ens<NT, false, true> : k_ens<NT, false, false>;
+  if (sm) return mixed ? k_ens<NT, true, true, MINB> : k_ens<NT, true, false, MINB>;
+  return mixed ? k_ens<NT, false, true, MINB> : k_ens<NT, false, false, MINB>;
 }
 
-static EnsKernel kernel_for(int nt, bool sm, bool mixed) {
-  switch (nt) {
-    case 128: return pick<128>(sm, mixed);
-    case 512: return pick<512>(sm, mixed);
-    case 1024: return pick<1024>(sm, mixed);
-    default: return pick<256>(sm, mixed);
+// a block shape: threads per CTA, with CLMD_ENS_LEAN for the 64-register
+// variant (128, 256 and 512 threads)
+static int shape_threads(int shape) { return shape & 0xffff; }
+
+static EnsKernel kernel_for(int shape, bool sm, bool mixed) {
+  const bool lean = (shape & CLMD_ENS_LEAN) != 0;
+  switch (shape_threads(shape)) {
+    case 128: return lean ? pick<128, 8>(sm, mixed) : pick<128, 4>(sm, mixed);
+    case 512: return lean ? pick<512, 2>(sm, mixed) : pick<512, 1>(sm, mixed);
+    case 1024: return pick<1024, 1>(sm, mixed);
+    default: return lean ? pick<256, 4>(sm, mixed) : pick<256, 2>(sm, mixed);
   }
 }
 
@@ -1337,11 +1355,12 @@ struct ClassLaunch {
   int grid = 0, nt = 0, ncmax = 1, item0 = 0, nitems = 0;
 };
 
-static int prepare_class(clmd_ensemble* E, int item0, int nitems, const int* slots, int nt,
+static int prepare_class(clmd_ensemble* E, int item0, int nitems, const int* slots, int shape,
                          ClassLaunch& L) {
   L = ClassLaunch();
   L.item0 = item0;
   L.nitems = nitems;
+  const int nt = shape_threads(shape);
   L.nt = nt;
   if (nitems == 0) return CLMD_OK;
   const bool mixed = E->cfg.precision == CLMD_PREC_MIXED;
@@ -1356,7 +1375,7 @@ static int prepare_class(clmd_ensemble* E, int item0, int nitems, const int* slo
     L.smem = std::max(L.smem, smem_bytes(R.natom, R.ncmax, sm));
     L.ncmax = std::max(L.ncmax, R.ncmax);
   }
-  L.k = kernel_for(nt, sm, mixed);
+  L.k = kernel_for(shape, sm, mixed);
   // the attribute only grows: classes that share a kernel may launch it
   // with different amounts in one sequence (occupancy follows each launch)
   size_t& lim = E->attr_smem[(void*)L.k];
@@ -1399,13 +1418,16 @@ static int enqueue_class(clmd_ensemble* E, int c, const ClassLaunch& L, int nwin
 // steps, t_i its device time per step measured in its earlier launches, so
 // that every CTA stays busy about min_ms whatever its replica's size (a
 // replica not yet timed runs a few steps)
-static int launch_all(clmd_ensemble* E, int nwin, const int* threads, float min_ms = 0.0f) {
+// only >= 0: that size class alone (the autotuner's trials)
+static int launch_all(clmd_ensemble* E, int nwin, const int* threads, float min_ms = 0.0f,
+                      int only = -1) {
   std::vector<int> cls[clmd_ensemble::kClasses];
   int nmax[clmd_ensemble::kClasses] = {};
   for (int s = 0; s < E->cfg.max_replicas; s++)
     if (E->used[s] && !E->h_summary[s].x && !E->h_summary[s].y) {
       int n = E->h_reps[s].natom, c = 0;
       while (c < clmd_ensemble::kClasses - 1 && n > E->cls_max[c]) c++;
+      if (only >= 0 && c != only) continue;
       cls[c].push_back(s);
       nmax[c] = std::max(nmax[c], n);
     }
@@ -1430,6 +1452,10 @@ static int launch_all(clmd_ensemble* E, int nwin, const int* threads, float min_
     ECK(cudaMemcpyAsync(E->d_iwin, E->h_iwin, sizeof(int) * total, cudaMemcpyHostToDevice,
                         E->stream));
   }
+  for (int c = 0; c < clmd_ensemble::kClasses; c++) {
+    E->last_ms[c] = -1.0f;
+    E->last_atoms[c] = 0;
+  }
   if (total == 0) return CLMD_OK;
   ClassLaunch L[clmd_ensemble::kClasses];
   std::vector<long long> key;
@@ -1441,7 +1467,6 @@ static int launch_all(clmd_ensemble* E, int nwin, const int* threads, float min_
   {
     int off = 0;
     for (int c = 0; c < clmd_ensemble::kClasses; c++) {
-      E->last_atoms[c] = 0;
       for (int s : cls[c]) E->last_atoms[c] += E->h_reps[s].natom;
       int st = prepare_class(E, off, (int)cls[c].size(), cls[c].data(), threads[c], L[c]);
       if (st) return st;
@@ -1512,23 +1537,29 @@ static int launch_all(clmd_ensemble* E, int nwin, const int* threads, float min_
   return CLMD_OK;
 }
 
-// Picks the block size of each size class from {128, 256, 512, 1024} by
-// timing one window per candidate on the running replicas (the trial
-// windows advance the simulation like any other window).
+// Picks the block shape of each size class from 128, 256, 512 and 1024
+// threads (<= 128 registers per thread below 1024) and the register-lean
+// 128, 256 and 512 (64 registers: 8, 4 and 2 CTAs per SM where shared
+// memory allows) by timing one window per candidate and class on the
+// running replicas, each class alone (the classes share the GPU when they
+// run together, and the window then takes about the sum of their times
+// alone; the trial windows advance the simulation like any other window).
 static int autotune(clmd_ensemble* E) {
-  const int cand[4] = {128, 256, 512, 1024};
+  constexpr int kCand = 7;
+  const int cand[kCand] = {128, 256, 512, 1024, 128 | CLMD_ENS_LEAN, 256 | CLMD_ENS_LEAN,
+                           512 | CLMD_ENS_LEAN};
   float best[clmd_ensemble::kClasses];
   int pick[clmd_ensemble::kClasses];
   for (int c = 0; c < clmd_ensemble::kClasses; c++) {
     best[c] = 1e30f;
     pick[c] = E->cls_threads[c];
   }
-  for (int k = 0; k < 4; k++) {
+  for (int k = 0; k < kCand; k++) {
     int th[clmd_ensemble::kClasses];
     for (int c = 0; c < clmd_ensemble::kClasses; c++) th[c] = cand[k];
-    int st = launch_all(E, 1, th);
-    if (st) return st;
     for (int c = 0; c < clmd_ensemble::kClasses; c++) {
+      int st = launch_all(E, 1, th, 0.0f, c);
+      if (st) return st;
       if (E->last_ms[c] < 0 || E->last_atoms[c] == 0) continue;
       float per_atom = E->last_ms[c] / (float)E->last_atoms[c];
       if (per_atom < best[c]) {

@@ -236,7 +236,7 @@ typedef struct clmd_ens_config {
   int32_t integrator;            /* CLMD_INT_VERLET or CLMD_INT_NOSE */
   int32_t ftcsi;                 /* steps per window (between cluster analyses) */
   int32_t nbtim;                 /* target steps between list rebuilds */
-  int32_t threads;               /* threads per replica (CTA size); 0 = autotune */
+  int32_t threads;               /* threads per replica (CTA size, | CLMD_ENS_LEAN); 0 = autotune */
   int32_t pad;
 } clmd_ens_config;
 
@@ -286,12 +286,18 @@ int clmd_ens_step(clmd_ensemble* e, int32_t nwin);
  * fall inside a window: the analysis still runs at every multiple of ftcsi,
  * and trajectories are those of clmd_ens_step. */
 int clmd_ens_step_timed(clmd_ensemble* e, float ms);
-/* Autotuner: picks the block size of each of the 4 replica-size classes
- * (atoms <= 1536, <= 3072, <= 6144, larger) from {128, 256, 512, 1024} by
- * timing one window per candidate on the running replicas; those 4 windows
- * advance the simulation.  threads_out (4 entries, may be NULL) gets the
- * choice.  Without it the classes use 128/256/512/1024 threads, or
- * clmd_ens_config.threads for all if that is set. */
+/* Block shape flag: the register-lean variant of a 128-, 256- or 512-thread
+ * CTA (64 registers per thread, so 8, 4 or 2 CTAs fit per SM where shared
+ * memory allows; the plain shapes allow up to 128 registers below 1024
+ * threads). */
+#define CLMD_ENS_LEAN 0x10000
+/* Autotuner: picks the block shape of each of the 4 replica-size classes
+ * (atoms <= 2048, <= 4096, <= 6144, larger) from 128, 256, 512, 1024 and
+ * the CLMD_ENS_LEAN 128, 256 and 512 by timing one window per candidate and
+ * class, each class alone on the GPU, on the running replicas; every replica
+ * advances by those 7 windows.  threads_out (4 entries, may be NULL) gets the choice (threads
+ * in the low 16 bits).  Without it the classes use 128/256/512/1024 threads,
+ * or clmd_ens_config.threads for all if that is set (the flag allowed). */
 int clmd_ens_autotune(clmd_ensemble* e, int32_t* threads_out);
 /* Per-slot results of all occupied slots (n gets the count). */
 int clmd_ens_results(clmd_ensemble* e, clmd_replica_result* out, int32_t cap, int32_t* n);
