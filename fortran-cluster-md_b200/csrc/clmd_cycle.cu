@@ -972,11 +972,34 @@ __global__ void __launch_bounds__(kPB, CLMD_CYCLE_MINB) k_cycle(Params P, DevSta
             __syncthreads();
             goto done;
           }
+          // v = W c, fused with the next step's drift (the same expressions
+          // as the drift at the top of the step, PSI = pn) unless this is the
+          // launch's last step or velocities are rescaled before each step
           const double c = 1.0 / (1.0 + dth * pn);
+          const bool fuse = !thermo && !last;
+          double d2 = 0.0, sv = 0.0;
+          double4* pos = posb[cur];
           for (int p = t0; p < N; p += G) {
-            A.vx[p] = A.vx[p] * c;
-            A.vy[p] = A.vy[p] * c;
-            A.vz[p] = A.vz[p] * c;
+            double vxi = A.vx[p] * c, vyi = A.vy[p] * c, vzi = A.vz[p] * c;
+            if (fuse) {
+              double axi = A.ax[p], ayi = A.ay[p], azi = A.az[p];
+              double dx = dt * vxi + dt2 * (axi - pn * vxi);
+              double dy = dt * vyi + dt2 * (ayi - pn * vyi);
+              double dz = dt * vzi + dt2 * (azi - pn * vzi);
+              sv = sv + vxi * vxi + vyi * vyi + vzi * vzi;
+              vxi = vxi + dth * (axi - pn * vxi);
+              vyi = vyi + dth * (ayi - pn * vyi);
+              vzi = vzi + dth * (azi - pn * vzi);
+              double4 q = pos[p];
+              q.x = q.x + dx;
+              q.y = q.y + dy;
+              q.z = q.z + dz;
+              pos[p] = q;
+              d2 = fmax(d2, dx * dx + dy * dy + dz * dz);
+            }
+            A.vx[p] = vxi;
+            A.vy[p] = vyi;
+            A.vz[p] = vzi;
           }
           if (threadIdx.x == 0) {
             B.q.nh_iters = 1;
@@ -984,8 +1007,16 @@ __global__ void __launch_bounds__(kPB, CLMD_CYCLE_MINB) k_cycle(Params P, DevSta
             B.q.psi = pn;
             B.q.ekin = 0.5 * m * B.q.sumv2;
           }
-          __syncthreads();
-          drift_done = false;
+          if (fuse) {
+            // the forces' reads of pos ended at the barrier before the root
+            put_max(red(), SLOT_MAX, d2, sh);
+            put_sum(red(), SLOT_SUMV2, sv, sh);
+            if (!gbar(st)) goto timeout;
+            drift_done = true;
+          } else {
+            __syncthreads();
+            drift_done = false;
+          }
           continue;
         }
         double psn = psi;

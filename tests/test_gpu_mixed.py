@@ -137,6 +137,32 @@ def test_mixed_nose_hoover_step_against_oracle_sweeps(gpu):
     g.close()
 
 
+def test_mixed_nose_hoover_launch_same_as_single_steps(gpu):
+    """Inside one launch the mixed Nose-Hoover step scales v = W / (1 + dth
+    PSI) in the same pass as the next step's drift; a launch's last step
+    scales alone and the next launch drifts first.  Both orders evaluate the
+    same expressions: 60 steps in one launch and 60 one-step launches give
+    bit-identical states (rebuilds included)."""
+    cfg = nvt_config(20000, clmd.PREC_MIXED, ftcsi=0)
+    st = random_state(cfg, 5)
+    out = []
+    for per_step in (False, True):
+        g = start(cfg, st.copy())
+        if per_step:
+            for step in range(1, 61):
+                g.integrator(step)
+        else:
+            g.steps(1, 60)
+        s = g.scalars()
+        assert s.status == 0 and s.nrebuild >= 2
+        out.append((g.get_state(), s))
+        g.close()
+    (a, sa), (b, sb) = out
+    for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az"):
+        assert np.array_equal(getattr(a, k), getattr(b, k)), k
+    assert (sa.psi, sa.s, sa.ekin, sa.atrskin) == (sb.psi, sb.s, sb.ekin, sb.atrskin)
+
+
 def test_mixed_energy_drift_tracks_fp64(gpu):
     """H = ekin + epot + Q PSI^2 / 2 + 3 N kT s over 1e4 Nose-Hoover steps.
     The truncated (unshifted) LJ of the reference loses energy whenever a pair
