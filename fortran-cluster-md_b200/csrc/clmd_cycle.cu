@@ -25,7 +25,7 @@
 #include <cuda_runtime.h>
 #include <stdio.h>
 
-#include "clmd_nh.cuh"
+#include "clmd_mixed.cuh"
 #include "clmd_system.hpp"
 
 namespace clmd {

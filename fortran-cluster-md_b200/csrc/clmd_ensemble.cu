@@ -32,7 +32,7 @@
 #include <vector>
 
 #include "../../include/clmd.h"
-#include "clmd_nh.cuh"
+#include "clmd_mixed.cuh"
 
 namespace clmd_ens {
 
@@ -443,7 +443,7 @@ __device__ void forces(Rep& R, Cta& C, const Args& A, const Pos<SM>& P, bool kic
         double r2d = dx * dx + dy * dy + dz * dz;
         if (r2d <= rc2) {
           float r2 = (float)r2d;
-          float ri2 = __frcp_rn(r2);
+          float ri2 = clmd_rcp_f32(r2);
           float r6 = ri2 * ri2 * ri2;
           float fij = 48.0f * ri2 * r6 * (r6 - 0.5f);
           kahan(fx, cx, fij * (float)dx);

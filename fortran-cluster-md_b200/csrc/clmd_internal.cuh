@@ -19,6 +19,8 @@
 
 #include "../../include/clmd.h"
 
+#include "clmd_mixed.cuh"
+
 namespace clmd {
 
 constexpr int kBlock = 256;        // threads per block of the per-atom kernels
@@ -182,7 +184,7 @@ __device__ __forceinline__ void pair_term_f32(const Params& P, int ij, double r2
                                               double dy, double dz, double& tx, double& ty,
                                               double& tz, double& e, double& w) {
   const float r2 = (float)r2d;
-  const float ri2 = 1.0f / r2;
+  const float ri2 = clmd_rcp_f32(r2);
   const float r6 = ri2 * ri2 * ri2;
   const float eps = (float)P.eps[ij], c1 = (float)P.c1[ij], c2 = (float)P.c2[ij],
               c3 = (float)P.c3[ij];

@@ -1,8 +1,19 @@
-// Closed-form Nose-Hoover velocity solve shared by the mixed-precision
-// kernels (k_cycle, k_ens).
+// Device helpers shared by the mixed-precision kernels (k_cycle, k_force,
+// k_ens): the FP32 reciprocal of the pair terms and the closed-form
+// Nose-Hoover velocity solve.
 #pragma once
 
 #include <math.h>
+
+// 1/x by the hardware's approximate reciprocal (PTX rcp.approx.ftz.f32, at
+// most 1 ulp from the exact quotient): x = r^2 of a pair inside the cut-off,
+// a normal number.  The pair terms are FP32 anyway; the IEEE-rounded
+// division costs several instructions more per pair.
+__device__ __forceinline__ float clmd_rcp_f32(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
 
 // The implicit Nose-Hoover velocity step of int-verlet-nh-mav.f:105-147 in
 // closed form (mixed precision).  The reference's Newton sweeps stop at the
