@@ -44,9 +44,15 @@ def force_errors(st, ref):
     return norm, per_atom
 
 
-@pytest.mark.parametrize("precision,tol", [(clmd.PREC_MIXED, 1e-5), (clmd.PREC_FP64, 1e-12)])
-def test_ensemble_forces_against_oracle(gpu, precision, tol):
-    e = clmd.Ensemble(clmd.ens_config(20000, 8, precision=precision, ftcsi=50))
+@pytest.mark.parametrize("precision,tol,threads", [
+    (clmd.PREC_MIXED, 1e-5, 0), (clmd.PREC_FP64, 1e-12, 0),
+    (clmd.PREC_MIXED, 1e-5, 256 | clmd.ENS_LEAN), (clmd.PREC_MIXED, 1e-5, 512 | clmd.ENS_LEAN),
+    (clmd.PREC_FP64, 1e-12, 128 | clmd.ENS_LEAN)])
+def test_ensemble_forces_against_oracle(gpu, precision, tol, threads):
+    """Every block shape the autotuner may pick (the default per-class
+    shapes and the register-lean ones) against the FP64 oracle."""
+    e = clmd.Ensemble(clmd.ens_config(20000, 8, precision=precision, ftcsi=50,
+                                      threads=threads))
     slots = []
     for k, (n, rho) in enumerate([(1500, 0.05), (800, 0.02), (3000, 0.3)]):
         box, arrs = replica_inputs(n, rho, 0.75, 100 + k)
@@ -90,6 +96,14 @@ def test_mixed_ensemble_nose_hoover_tracks_fp64(gpu):
         dek = abs(ra.ekin - rb.ekin) / rb.ekin
         print(f"N={n}: dv {dv:.2e} dpsi {dpsi:.2e} dekin {dek:.2e}")
         assert dv <= 1e-6 and dpsi <= 1e-6 and dek <= 1e-6, (n, dv, dpsi, dek)
+
+
+def test_unsupported_block_shape_rejected(gpu):
+    """Only the compiled shapes are accepted (a kernel launched with another
+    block size would index its per-warp buffers out of range)."""
+    for bad in (300, 64, 1024 | clmd.ENS_LEAN, -1):
+        with pytest.raises(clmd.ClmdError):
+            clmd.Ensemble(clmd.ens_config(4000, 2, threads=bad))
 
 
 def test_ensemble_cluster_labels_exact(gpu):
