@@ -139,6 +139,33 @@ __device__ __forceinline__ void cta_sum2(double& a, double& b, int& f, double* s
   __syncthreads();
 }
 
+// the block sum of S (the tree of cta_sum2) and the closed-form Nose-Hoover
+// root (clmd_nh_root) on warp 0 alone, published by the second barrier:
+// the other warps skip the scalar Newton steps and their divisions
+template <int NT>
+__device__ __forceinline__ bool cta_nh_root(double S, double psi1, double nkt3, double dth,
+                                            double Q, double* sh, double& Stot, double& p) {
+  constexpr int W = NT / 32;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  S = wsum(S);
+  if (lane == 0) sh[w] = S;
+  __syncthreads();
+  if (w == 0) {
+    const double t = wsum(lane < W ? sh[lane] : 0.0);
+    double pr;
+    const bool ok = clmd_nh_root(t, psi1, nkt3, dth, Q, pr);
+    if (lane == 0) {
+      sh[32] = t;
+      sh[33] = pr;
+      sh[34] = ok ? 1.0 : 0.0;
+    }
+  }
+  __syncthreads();
+  Stot = sh[32];
+  p = sh[33];
+  return sh[34] != 0.0;
+}
+
 // block max of a and sum of b in one round (as cta_sum2)
 template <int NT>
 __device__ __forceinline__ void cta_maxsum(double& a, double& b, double* sh) {
@@ -817,10 +844,8 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
         const double Q = R.Q, err = 1.0e-10, psi1 = R.psi, dtQ = dt / Q;
         if (MIXED) {
           double S = 0.0, unused = 0.0, p;
-          int nr0 = 0;
           forces<NT, SM, MIXED, true>(R, C, A, P, false, last, psi1, dtQ, &S, &unused);
-          cta_sum2<NT>(S, unused, nr0, C.red);
-          if (!clmd_nh_root(S, psi1, R.nkt3_i, dth, Q, p)) {
+          if (!cta_nh_root<NT>(S, psi1, R.nkt3_i, dth, Q, C.red, S, p)) {
             if (tid == 0 && R.status == 0) R.status = CLMD_ERR_NH_NOCONVERGE;
             __syncthreads();
             goto out;
