@@ -460,6 +460,7 @@ __device__ void forces(Rep& R, Cta& C, const Args& A, const Pos<SM>& P, bool kic
       // the next row entry is loaded while this pair is evaluated
       const int* lp = A.list + lbase + i;
       int jn = len > 0 ? lp[0] : 0;
+#pragma unroll 2
       for (int k = 0; k < len; k++) {
         const int j = jn;
         lp += N;
