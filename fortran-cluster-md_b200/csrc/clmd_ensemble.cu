@@ -50,6 +50,9 @@ struct Rep {
   double dmmh[256];
   int dmmst, dmmi, step, status, done, clbrkt, maxcs, fpt_top, nrebuild, cstep, started;
   int ncmax;  // cell-grid cap, fixed at admission from this replica's size only
+  // positions too large for shared memory: the atoms are kept in cell order
+  // (rebuild) and orig[] holds each slot's atom number (fixed at admission)
+  int reorder;
 };
 
 struct Args {
@@ -58,6 +61,7 @@ struct Args {
   void* a;  // float[3][pool] (mixed) or double[3][pool] (FP64)
   long long pool;
   int *list, *rlen, *sorted, *cellid, *parent, *cs, *cl, *fpt;
+  int* orig;  // per slot: the atom number it holds (replicas with reorder set)
   Rep* reps;
   const int* items;
   const int* iwin;  // MD steps per item (nullptr: nwin windows for every item)
@@ -352,6 +356,43 @@ __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
     A.sorted[off + c0 + r] = i;
   }
   __syncthreads();
+  if (!SM && R.reorder) {
+    // positions in global memory: the atoms move into cell order, so that a
+    // warp's neighbour gathers fall within a few cells' worth of memory.
+    // vn and parent[] are dead here (the force pass and the analysis
+    // rewrite them), so they hold the gathered copies.  Accelerations are
+    // dead too: the force pass after a rebuild writes them before any read.
+    const int* srt = A.sorted + off;
+    double *gx = A.vxn + off, *gy = A.vyn + off, *gz = A.vzn + off;
+    int* go = A.parent + off;
+    for (int p = tid; p < N; p += NT) {
+      const int q = srt[p];
+      gx[p] = P.x(q);
+      gy[p] = P.y(q);
+      gz[p] = P.z(q);
+      go[p] = A.orig[off + q];
+    }
+    __syncthreads();
+    for (int p = tid; p < N; p += NT) {
+      P.set(p, gx[p], gy[p], gz[p]);
+      A.orig[off + p] = go[p];
+    }
+    __syncthreads();
+    for (int p = tid; p < N; p += NT) {
+      const int q = srt[p];
+      gx[p] = A.vx[off + q];
+      gy[p] = A.vy[off + q];
+      gz[p] = A.vz[off + q];
+    }
+    __syncthreads();
+    for (int p = tid; p < N; p += NT) {
+      A.vx[off + p] = gx[p];
+      A.vy[off + p] = gy[p];
+      A.vz[off + p] = gz[p];
+      A.sorted[off + p] = p;  // the cells now hold consecutive slots
+    }
+    __syncthreads();
+  }
   const double hL = 0.5 * L, rs2 = C.rs2;
   const long long lbase = (long long)off * A.lstride;
   int over = 0;
@@ -670,10 +711,26 @@ __device__ void analysis(Rep& R, Cta& C, const Args& A, const Pos<SM>& P, int st
     }
   }
   __syncthreads();
-  for (int i = tid; i < N; i += NT) {
-    int r = ufind(par, i);
-    A.cl[off + i] = r + 1;
-    atomicAdd(cs + r, 1);
+  if (R.reorder) {
+    // slots are in cell order: a cluster's label is the smallest atom number
+    // (orig) among its slots, as for atoms kept in their own order.  sorted[]
+    // is free outside the rebuild.
+    int* mo = A.sorted + off;
+    for (int i = tid; i < N; i += NT) mo[i] = 0x7fffffff;
+    __syncthreads();
+    for (int i = tid; i < N; i += NT) atomicMin(mo + ufind(par, i), A.orig[off + i]);
+    __syncthreads();
+    for (int i = tid; i < N; i += NT) {
+      int r = ufind(par, i);
+      A.cl[off + A.orig[off + i]] = mo[r] + 1;  // by atom number: slots move at rebuilds
+      atomicAdd(cs + r, 1);
+    }
+  } else {
+    for (int i = tid; i < N; i += NT) {
+      int r = ufind(par, i);
+      A.cl[off + i] = r + 1;
+      atomicAdd(cs + r, 1);
+    }
   }
   __syncthreads();
   double m = 0.0;
@@ -1161,6 +1218,7 @@ extern "C" int clmd_ens_create(const clmd_ens_config* cfg, clmd_ensemble** out) 
   ECK(cudaMalloc(&A.rlen, 4 * P)); ECK(cudaMalloc(&A.sorted, 4 * P));
   ECK(cudaMalloc(&A.cellid, 4 * P)); ECK(cudaMalloc(&A.parent, 4 * P));
   ECK(cudaMalloc(&A.cs, 4 * P)); ECK(cudaMalloc(&A.cl, 4 * P));
+  ECK(cudaMalloc(&A.orig, 4 * P));
   ECK(cudaMemset(A.a, 0, 3 * 8 * P));
   ECK(cudaMemset(A.rlen, 0, 4 * P));
   ECK(cudaMemset(A.cl, 0, 4 * P));
@@ -1204,7 +1262,7 @@ extern "C" int clmd_ens_destroy(clmd_ensemble* E) {
   cudaStreamSynchronize(E->stream);
   Args& A = E->A;
   void* ps[] = {A.x, A.y, A.z, A.vx, A.vy, A.vz, A.vxn, A.vyn, A.vzn, A.a, A.list, A.rlen,
-                A.sorted, A.cellid, A.parent, A.cs, A.cl, A.reps, A.fpt, A.summary,
+                A.sorted, A.cellid, A.parent, A.cs, A.cl, A.orig, A.reps, A.fpt, A.summary,
                 E->d_items, E->d_ctr, E->d_iwin, A.wtime};
   for (void* p : ps)
     if (p) cudaFree(p);
@@ -1321,6 +1379,10 @@ extern "C" int clmd_ens_add(clmd_ensemble* E, const clmd_replica_spec* sp, const
   // the cell grid never needs more than box / rc cells per dimension (the
   // list radius stays above rc): small boxes keep their shared memory small
   R.ncmax = std::max(1, std::min(cells_for(E->smem_cap, N, &fits), (int)(sp->box / E->cfg.rc)));
+  R.reorder = fits ? 0 : 1;
+  std::vector<int> iota(N);
+  for (int i = 0; i < N; i++) iota[i] = i;
+  ECK(cudaMemcpyAsync(A.orig + off, iota.data(), 4 * (size_t)N, cudaMemcpyHostToDevice, st));
   ECK(cudaMemcpyAsync(A.reps + s, &R, sizeof(Rep), cudaMemcpyHostToDevice, st));
   E->h_summary[s] = make_int4(0, 0, 0, 0);
   ECK(cudaMemcpyAsync(A.summary + s, &E->h_summary[s], sizeof(int4), cudaMemcpyHostToDevice,
@@ -1687,6 +1749,23 @@ extern "C" int clmd_ens_poll(clmd_ensemble* E, clmd_replica_result* out, int32_t
   return CLMD_OK;
 }
 
+// the atom number each slot of a reordered replica holds (orig[])
+static int slot_orig(clmd_ensemble* E, int slot, std::vector<int>& o) {
+  const int N = E->h_reps[slot].natom;
+  o.resize(N);
+  ECK(cudaMemcpyAsync(o.data(), E->A.orig + E->slot_off[slot], 4 * (size_t)N,
+                      cudaMemcpyDeviceToHost, E->stream));
+  ECK(cudaStreamSynchronize(E->stream));
+  return CLMD_OK;
+}
+
+// a[p] (slot order) -> a[o[p]] (atom order)
+template <typename T>
+static void unpermute(T* a, const std::vector<int>& o) {
+  std::vector<T> t(a, a + o.size());
+  for (size_t p = 0; p < o.size(); p++) a[o[p]] = t[p];
+}
+
 extern "C" int clmd_ens_get_state(clmd_ensemble* E, int32_t slot, double* x, double* y,
                                   double* z, double* vx, double* vy, double* vz, double* ax,
                                   double* ay, double* az, int32_t* cl) {
@@ -1718,6 +1797,14 @@ extern "C" int clmd_ens_get_state(clmd_ensemble* E, int32_t slot, double* x, dou
   }
   if (cl) ECK(cudaMemcpyAsync(cl, A.cl + off, 4 * N, cudaMemcpyDeviceToHost, st));
   ECK(cudaStreamSynchronize(st));
+  if (E->h_reps[slot].reorder) {  // slots in cell order: back to atom order
+    std::vector<int> o;
+    int rc = slot_orig(E, slot, o);
+    if (rc) return rc;
+    double* arr[9] = {x, y, z, vx, vy, vz, ax, ay, az};
+    for (double* a : arr)
+      if (a) unpermute(a, o);  // (labels are stored by atom number already)
+  }
   return CLMD_OK;
 }
 
@@ -1826,6 +1913,25 @@ extern "C" int clmd_ens_upload(clmd_ensemble* E, const double* x, const double* 
     }
   }
   ECK(cudaStreamSynchronize(E->stream));
+  // reordered replicas: their slots take the atoms orig[] names
+  long long h = 0;
+  for (int s = 0; s < E->cfg.max_replicas; s++) {
+    if (!E->used[s]) continue;
+    const int n = E->h_reps[s].natom;
+    if (E->h_reps[s].reorder) {
+      std::vector<int> o;
+      int rc = slot_orig(E, s, o);
+      if (rc) return rc;
+      std::vector<double> t(n);
+      for (int k = 0; k < 6; k++) {
+        if (!src[k]) continue;
+        for (int p = 0; p < n; p++) t[p] = src[k][h + o[p]];
+        ECK(cudaMemcpy(dst[k] + E->slot_off[s], t.data(), 8 * (size_t)n,
+                       cudaMemcpyHostToDevice));
+      }
+    }
+    h += n;
+  }
   return CLMD_OK;
 }
 
@@ -1847,6 +1953,20 @@ extern "C" int clmd_ens_download(clmd_ensemble* E, double* x, double* y, double*
     }
   }
   ECK(cudaStreamSynchronize(E->stream));
+  // reordered replicas: back to atom order
+  long long h = 0;
+  for (int s = 0; s < E->cfg.max_replicas; s++) {
+    if (!E->used[s]) continue;
+    const int n = E->h_reps[s].natom;
+    if (E->h_reps[s].reorder) {
+      std::vector<int> o;
+      int rc = slot_orig(E, s, o);
+      if (rc) return rc;
+      for (int k = 0; k < 6; k++)
+        if (dst[k]) unpermute(dst[k] + h, o);
+    }
+    h += n;
+  }
   return CLMD_OK;
 }
 

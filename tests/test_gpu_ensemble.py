@@ -126,13 +126,43 @@ def test_ensemble_cluster_labels_exact(gpu):
     assert o.clusters()["cs"].max() > 2
 
 
-def test_replica_same_alone_and_in_mix(gpu):
-    n, rho, temp = 2000, 0.04, 0.7
+def test_reordered_replica_against_oracle(gpu):
+    """A replica whose positions do not fit in shared memory keeps its atoms
+    in cell order (reordered at every rebuild).  Seen through the API it is
+    in atom order: labels (the smallest atom number of each cluster) bit-exact
+    and mixed forces within 1e-5 against the oracle on the positions it
+    reports, after several windows of reordering."""
+    e = clmd.Ensemble(clmd.ens_config(30000, 2, ftcsi=20))
+    n, rho = 12000, 0.3
+    box, arrs = replica_inputs(n, rho, 0.7, 8)
+    slot = e.add(n, box, 0.7, *arrs)
+    e.step(3)
+    st, _ = e.state(slot)  # positions at the next analysis step
+    e.step(1)
+    _, cl = e.state(slot)  # labels of that analysis
+    res = e.results()[slot]
+    assert res.status == 0 and res.nrebuild >= 3
+    cfg = clmd.lj_config(n, rho, 0.7)
+    o = orc.Oracle(cfg, neighbor_mode=1)
+    z0 = np.zeros(n)
+    o.set_state(clmd.State(st.x, st.y, st.z, z0, z0, z0, z0, z0, z0),
+                scalars=orc.scalars_init(cfg))
+    o.neighbor(0)
+    o.stoddard(0)
+    assert np.array_equal(cl, o.clusters()["cl"])
+    assert o.clusters()["cs"].max() > 2
+    norm, per_atom = force_errors(st, oracle_forces(n, box, st).get_state())
+    assert norm <= 1e-5 and per_atom <= 1e-4, (norm, per_atom)
+
+
+@pytest.mark.parametrize("n", [2000, 11000])  # 11000: reordered slots
+def test_replica_same_alone_and_in_mix(gpu, n):
+    rho, temp = 0.04, 0.7
     box, arrs = replica_inputs(n, rho, temp, 42)
-    alone = clmd.Ensemble(clmd.ens_config(4000, 2, ftcsi=25, threads=256))
+    alone = clmd.Ensemble(clmd.ens_config(n + 2000, 2, ftcsi=25, threads=256))
     sa = alone.add(n, box, temp, *arrs, csover=51, budget=400)
     alone.step(4)
-    mix = clmd.Ensemble(clmd.ens_config(60000, 40, ftcsi=25, threads=256))
+    mix = clmd.Ensemble(clmd.ens_config(60000 + n, 40, ftcsi=25, threads=256))
     others = []
     rng = np.random.default_rng(0)
     for k in range(20):
@@ -293,8 +323,8 @@ def test_bulk_upload_download_in_slot_order(gpu):
     order, whether the slots' pool ranges abut or not (a removal and a
     re-admission leave them out of order)."""
     import ctypes as C
-    e = clmd.Ensemble(clmd.ens_config(20000, 8, ftcsi=10, threads=256))
-    sizes = [1200, 700, 2500, 900]
+    e = clmd.Ensemble(clmd.ens_config(40000, 8, ftcsi=10, threads=256))
+    sizes = [1200, 700, 12000, 900]  # 12000: positions beyond shared memory, slots reordered
     slots = []
     for k, n in enumerate(sizes):
         box, arrs = replica_inputs(n, 0.03, 0.7, 300 + k)
