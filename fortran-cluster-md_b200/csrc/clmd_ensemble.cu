@@ -1104,7 +1104,8 @@ struct clmd_ensemble {
   // size classes: each has its own block size, shared-memory budget, stream
   static constexpr int kClasses = 4;
   int cls_max[kClasses] = {2048, 4096, 6144, 1 << 30};  // measured best of a few splits
-  int cls_threads[kClasses] = {128, 256, 512, 1024};
+  // the shapes the autotuner picks on the batched workload (used until it runs)
+  int cls_threads[kClasses] = {512 | CLMD_ENS_LEAN, 1024, 1024, 1024};
   cudaStream_t cstream[kClasses] = {};
   cudaEvent_t ev0[kClasses] = {}, ev1[kClasses] = {}, evj = nullptr;
   cudaEvent_t evdone[kClasses] = {};  // join of each class stream

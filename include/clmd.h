@@ -296,8 +296,9 @@ int clmd_ens_step_timed(clmd_ensemble* e, float ms);
  * the CLMD_ENS_LEAN 128, 256 and 512 by timing one window per candidate and
  * class, each class alone on the GPU, on the running replicas; every replica
  * advances by those 7 windows.  threads_out (4 entries, may be NULL) gets the choice (threads
- * in the low 16 bits).  Without it the classes use 128/256/512/1024 threads,
- * or clmd_ens_config.threads for all if that is set (the flag allowed). */
+ * in the low 16 bits).  Without it the classes use lean 512, 1024, 1024 and
+ * 1024 threads (the tuner's picks on the batched workload), or
+ * clmd_ens_config.threads for all if that is set (the flag allowed). */
 int clmd_ens_autotune(clmd_ensemble* e, int32_t* threads_out);
 /* Per-slot results of all occupied slots (n gets the count). */
 int clmd_ens_results(clmd_ensemble* e, clmd_replica_result* out, int32_t cap, int32_t* n);
