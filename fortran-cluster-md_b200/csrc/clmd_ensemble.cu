@@ -1927,12 +1927,15 @@ extern "C" int clmd_ens_upload(clmd_ensemble* E, const double* x, const double* 
       for (int k = 0; k < 6; k++) {
         if (!src[k]) continue;
         for (int p = 0; p < n; p++) t[p] = src[k][h + o[p]];
-        ECK(cudaMemcpy(dst[k] + E->slot_off[s], t.data(), 8 * (size_t)n,
-                       cudaMemcpyHostToDevice));
+        // on the ensemble's stream (ordered before its next launch); a
+        // pageable source is staged before the call returns, so t is reusable
+        ECK(cudaMemcpyAsync(dst[k] + E->slot_off[s], t.data(), 8 * (size_t)n,
+                            cudaMemcpyHostToDevice, E->stream));
       }
     }
     h += n;
   }
+  ECK(cudaStreamSynchronize(E->stream));
   return CLMD_OK;
 }
 
