@@ -50,8 +50,9 @@ struct Rep {
   double dmmh[256];
   int dmmst, dmmi, step, status, done, clbrkt, maxcs, fpt_top, nrebuild, cstep, started;
   int ncmax;  // cell-grid cap, fixed at admission from this replica's size only
-  // positions too large for shared memory: the atoms are kept in cell order
-  // (rebuild) and orig[] holds each slot's atom number (fixed at admission)
+  // the atoms' order inside the engine, fixed at admission (orig[] maps each
+  // slot to its atom): 1 (positions too large for shared memory) cell order,
+  // 2 (the others) by the rows' lengths; both renewed at every rebuild
   int reorder;
 };
 
@@ -61,7 +62,7 @@ struct Args {
   void* a;  // float[3][pool] (mixed) or double[3][pool] (FP64)
   long long pool;
   int *list, *rlen, *sorted, *cellid, *parent, *cs, *cl, *fpt;
-  int* orig;  // per slot: the atom number it holds (replicas with reorder set)
+  int* orig;  // per slot: the pool index (offset + atom number) of the atom it holds
   Rep* reps;
   const int* items;
   const int* iwin;  // MD steps per item (nullptr: nwin windows for every item)
@@ -285,6 +286,70 @@ __device__ bool prologue(Rep& R, Cta& C, const Args& A, int step) {
   return true;
 }
 
+// reorder 2: new slot p <- old atom cs[p] (new slot of old atom i in
+// cellid[i]), a stable order (by index) of the atoms bucketed by their rows'
+// lengths at the last rebuild.  Per tile of NT atoms, warp ballots rank the
+// atoms of each bucket and the warps' counts (shared memory) place them.
+constexpr int kLenBuckets = 6;
+__device__ __forceinline__ int len_bucket(int len) {
+  return len <= 3 ? 0 : len <= 5 ? 1 : len <= 7 ? 2 : len <= 10 ? 3 : len <= 16 ? 4 : 5;
+}
+template <int NT>
+__device__ void length_order(const Rep& R, Cta& C, const Args& A) {
+  constexpr int W = NT / 32;
+  static_assert(W * kLenBuckets + kLenBuckets <= (int)(sizeof(C.red) / sizeof(int)),
+                "bucket counts fit the reduction scratch");
+  const int N = R.natom, off = R.off, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  int* cnt = (int*)C.red;           // [W][kLenBuckets]
+  int* base = cnt + W * kLenBuckets;  // [kLenBuckets]
+  // bucket sizes -> bucket starts
+  int mine[kLenBuckets] = {};
+  for (int i = tid; i < N; i += NT) mine[len_bucket(A.rlen[off + i])]++;
+#pragma unroll
+  for (int b = 0; b < kLenBuckets; b++) {
+    const int t = __reduce_add_sync(0xffffffffu, mine[b]);
+    if (lane == 0) cnt[w * kLenBuckets + b] = t;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int acc = 0;
+    for (int b = 0; b < kLenBuckets; b++) {
+      int t = 0;
+      for (int k = 0; k < W; k++) t += cnt[k * kLenBuckets + b];
+      base[b] = acc;
+      acc += t;
+    }
+  }
+  __syncthreads();
+  for (int i0 = 0; i0 < N; i0 += NT) {  // uniform: every thread takes every tile
+    const int i = i0 + tid;
+    const int key = i < N ? len_bucket(A.rlen[off + i]) : -1;
+    int rank = 0;
+#pragma unroll
+    for (int b = 0; b < kLenBuckets; b++) {
+      const unsigned m = __ballot_sync(0xffffffffu, key == b);
+      if (key == b) rank = __popc(m & lt);
+      if (lane == 0) cnt[w * kLenBuckets + b] = __popc(m);
+    }
+    __syncthreads();
+    if (key >= 0) {
+      int pre = base[key];
+      for (int k = 0; k < w; k++) pre += cnt[k * kLenBuckets + key];
+      const int slot = pre + rank;
+      A.cellid[off + i] = slot;
+      A.cs[off + slot] = i;
+    }
+    __syncthreads();
+    if (tid < kLenBuckets) {
+      int t = 0;
+      for (int k = 0; k < W; k++) t += cnt[k * kLenBuckets + tid];
+      base[tid] += t;
+    }
+    __syncthreads();
+  }
+}
+
 // cell list + rows (ELL, transposed per replica: entry k of atom i at
 // list[off*stride + k*N + i]); cells are index-sorted so row order is fixed
 template <int NT, bool SM>
@@ -356,13 +421,20 @@ __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
     A.sorted[off + c0 + r] = i;
   }
   __syncthreads();
-  if (!SM && R.reorder) {
-    // positions in global memory: the atoms move into cell order, so that a
-    // warp's neighbour gathers fall within a few cells' worth of memory.
+  if ((!SM && R.reorder == 1) || R.reorder == 2) {
+    // reorder 1 (positions in global memory): the atoms move into cell
+    // order, so that a warp's neighbour gathers fall within a few cells'
+    // worth of memory.  reorder 2: a stable order by the previous rows'
+    // lengths (bucketed), so that a warp's rows are of similar length and
+    // its lanes finish together (rows change little between rebuilds).
     // vn and parent[] are dead here (the force pass and the analysis
     // rewrite them), so they hold the gathered copies.  Accelerations are
     // dead too: the force pass after a rebuild writes them before any read.
     const int* srt = A.sorted + off;
+    if (R.reorder == 2) {
+      length_order<NT>(R, C, A);
+      srt = A.cs + off;
+    }
     double *gx = A.vxn + off, *gy = A.vyn + off, *gz = A.vzn + off;
     int* go = A.parent + off;
     for (int p = tid; p < N; p += NT) {
@@ -389,7 +461,10 @@ __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
       A.vx[off + p] = gx[p];
       A.vy[off + p] = gy[p];
       A.vz[off + p] = gz[p];
-      A.sorted[off + p] = p;  // the cells now hold consecutive slots
+      if (R.reorder == 2)
+        A.sorted[off + p] = A.cellid[off + A.sorted[off + p]];  // old index -> new slot
+      else
+        A.sorted[off + p] = p;  // the cells now hold consecutive slots
     }
     __syncthreads();
   }
@@ -718,11 +793,11 @@ __device__ void analysis(Rep& R, Cta& C, const Args& A, const Pos<SM>& P, int st
     int* mo = A.sorted + off;
     for (int i = tid; i < N; i += NT) mo[i] = 0x7fffffff;
     __syncthreads();
-    for (int i = tid; i < N; i += NT) atomicMin(mo + ufind(par, i), A.orig[off + i]);
+    for (int i = tid; i < N; i += NT) atomicMin(mo + ufind(par, i), A.orig[off + i] - off);
     __syncthreads();
     for (int i = tid; i < N; i += NT) {
       int r = ufind(par, i);
-      A.cl[off + A.orig[off + i]] = mo[r] + 1;  // by atom number: slots move at rebuilds
+      A.cl[A.orig[off + i]] = mo[r] + 1;  // by atom number: slots move at rebuilds
       atomicAdd(cs + r, 1);
     }
   } else {
@@ -1099,6 +1174,7 @@ struct clmd_ensemble {
   int* d_iwin = nullptr;   // windows per item (balanced launches)
   int* h_iwin = nullptr;   // pinned
   float* h_wtime = nullptr;  // pinned copy of A.wtime
+  double* d_stage = nullptr;  // bulk copies in atom order (pool doubles, on first use)
   int4* h_summary = nullptr;  // pinned copy of A.summary
   bool reps_stale = false;    // h_reps older than the device records
   // size classes: each has its own block size, shared-memory budget, stream
@@ -1264,7 +1340,7 @@ extern "C" int clmd_ens_destroy(clmd_ensemble* E) {
   Args& A = E->A;
   void* ps[] = {A.x, A.y, A.z, A.vx, A.vy, A.vz, A.vxn, A.vyn, A.vzn, A.a, A.list, A.rlen,
                 A.sorted, A.cellid, A.parent, A.cs, A.cl, A.orig, A.reps, A.fpt, A.summary,
-                E->d_items, E->d_ctr, E->d_iwin, A.wtime};
+                E->d_items, E->d_ctr, E->d_iwin, A.wtime, E->d_stage};
   for (void* p : ps)
     if (p) cudaFree(p);
   if (E->h_reps) cudaFreeHost(E->h_reps);
@@ -1380,10 +1456,11 @@ extern "C" int clmd_ens_add(clmd_ensemble* E, const clmd_replica_spec* sp, const
   // the cell grid never needs more than box / rc cells per dimension (the
   // list radius stays above rc): small boxes keep their shared memory small
   R.ncmax = std::max(1, std::min(cells_for(E->smem_cap, N, &fits), (int)(sp->box / E->cfg.rc)));
-  R.reorder = fits ? 0 : 1;
+  R.reorder = fits ? 2 : 1;  // (rows of similar length per warp; large: gathers near)
   std::vector<int> iota(N);
-  for (int i = 0; i < N; i++) iota[i] = i;
+  for (int i = 0; i < N; i++) iota[i] = (int)off + i;
   ECK(cudaMemcpyAsync(A.orig + off, iota.data(), 4 * (size_t)N, cudaMemcpyHostToDevice, st));
+  ECK(cudaMemsetAsync(A.rlen + off, 0, 4 * (size_t)N, st));  // the first order: pool history-free
   ECK(cudaMemcpyAsync(A.reps + s, &R, sizeof(Rep), cudaMemcpyHostToDevice, st));
   E->h_summary[s] = make_int4(0, 0, 0, 0);
   ECK(cudaMemcpyAsync(A.summary + s, &E->h_summary[s], sizeof(int4), cudaMemcpyHostToDevice,
@@ -1757,6 +1834,7 @@ static int slot_orig(clmd_ensemble* E, int slot, std::vector<int>& o) {
   ECK(cudaMemcpyAsync(o.data(), E->A.orig + E->slot_off[slot], 4 * (size_t)N,
                       cudaMemcpyDeviceToHost, E->stream));
   ECK(cudaStreamSynchronize(E->stream));
+  for (int& v : o) v -= (int)E->slot_off[slot];  // pool index -> atom number
   return CLMD_OK;
 }
 
@@ -1895,11 +1973,31 @@ static void host_ranges(clmd_ensemble* E, std::vector<std::pair<long long, long 
   }
 }
 
+// bulk copies in atom order: slot g holds pool index orig[g] (the replicas
+// that keep their atoms reordered move them, the others hold orig[g] = g)
+__global__ void k_from_atom_order(double* dst, const double* stage, const int* orig,
+                                  long long first, long long n) {
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) dst[first + k] = stage[orig[first + k]];
+}
+__global__ void k_to_atom_order(double* stage, const double* src, const int* orig,
+                                long long first, long long n) {
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) stage[orig[first + k]] = src[first + k];
+}
+
+static int ensure_stage(clmd_ensemble* E) {
+  if (!E->d_stage) ECK(cudaMalloc(&E->d_stage, 8 * (size_t)E->A.pool));
+  return CLMD_OK;
+}
+
 extern "C" int clmd_ens_upload(clmd_ensemble* E, const double* x, const double* y,
                                const double* z, const double* vx, const double* vy,
                                const double* vz) {
   if (!E) return CLMD_ERR_ARG;
   std::lock_guard<std::mutex> lock(E->mu);
+  int rc = ensure_stage(E);
+  if (rc) return rc;
   std::vector<std::pair<long long, long long>> r;
   host_ranges(E, r);
   const double* src[6] = {x, y, z, vx, vy, vz};
@@ -1908,32 +2006,15 @@ extern "C" int clmd_ens_upload(clmd_ensemble* E, const double* x, const double* 
     if (!src[k]) continue;
     long long h = 0;
     for (auto& q : r) {
-      ECK(cudaMemcpyAsync(dst[k] + q.first, src[k] + h, 8 * (size_t)q.second,
+      ECK(cudaMemcpyAsync(E->d_stage + q.first, src[k] + h, 8 * (size_t)q.second,
                           cudaMemcpyHostToDevice, E->stream));
+      const unsigned nb = (unsigned)((q.second + 255) / 256);
+      k_from_atom_order<<<nb, 256, 0, E->stream>>>(dst[k], E->d_stage, E->A.orig, q.first,
+                                                    q.second);
+      ECK(cudaGetLastError());
+      E->launches++;
       h += q.second;
     }
-  }
-  ECK(cudaStreamSynchronize(E->stream));
-  // reordered replicas: their slots take the atoms orig[] names
-  long long h = 0;
-  for (int s = 0; s < E->cfg.max_replicas; s++) {
-    if (!E->used[s]) continue;
-    const int n = E->h_reps[s].natom;
-    if (E->h_reps[s].reorder) {
-      std::vector<int> o;
-      int rc = slot_orig(E, s, o);
-      if (rc) return rc;
-      std::vector<double> t(n);
-      for (int k = 0; k < 6; k++) {
-        if (!src[k]) continue;
-        for (int p = 0; p < n; p++) t[p] = src[k][h + o[p]];
-        // on the ensemble's stream (ordered before its next launch); a
-        // pageable source is staged before the call returns, so t is reusable
-        ECK(cudaMemcpyAsync(dst[k] + E->slot_off[s], t.data(), 8 * (size_t)n,
-                            cudaMemcpyHostToDevice, E->stream));
-      }
-    }
-    h += n;
   }
   ECK(cudaStreamSynchronize(E->stream));
   return CLMD_OK;
@@ -1943,6 +2024,8 @@ extern "C" int clmd_ens_download(clmd_ensemble* E, double* x, double* y, double*
                                  double* vx, double* vy, double* vz) {
   if (!E) return CLMD_ERR_ARG;
   std::lock_guard<std::mutex> lock(E->mu);
+  int rc = ensure_stage(E);
+  if (rc) return rc;
   std::vector<std::pair<long long, long long>> r;
   host_ranges(E, r);
   double* dst[6] = {x, y, z, vx, vy, vz};
@@ -1951,26 +2034,17 @@ extern "C" int clmd_ens_download(clmd_ensemble* E, double* x, double* y, double*
     if (!dst[k]) continue;
     long long h = 0;
     for (auto& q : r) {
-      ECK(cudaMemcpyAsync(dst[k] + h, src[k] + q.first, 8 * (size_t)q.second,
+      const unsigned nb = (unsigned)((q.second + 255) / 256);
+      k_to_atom_order<<<nb, 256, 0, E->stream>>>(E->d_stage, src[k], E->A.orig, q.first,
+                                                  q.second);
+      ECK(cudaGetLastError());
+      E->launches++;
+      ECK(cudaMemcpyAsync(dst[k] + h, E->d_stage + q.first, 8 * (size_t)q.second,
                           cudaMemcpyDeviceToHost, E->stream));
       h += q.second;
     }
   }
   ECK(cudaStreamSynchronize(E->stream));
-  // reordered replicas: back to atom order
-  long long h = 0;
-  for (int s = 0; s < E->cfg.max_replicas; s++) {
-    if (!E->used[s]) continue;
-    const int n = E->h_reps[s].natom;
-    if (E->h_reps[s].reorder) {
-      std::vector<int> o;
-      int rc = slot_orig(E, s, o);
-      if (rc) return rc;
-      for (int k = 0; k < 6; k++)
-        if (dst[k]) unpermute(dst[k] + h, o);
-    }
-    h += n;
-  }
   return CLMD_OK;
 }
 
