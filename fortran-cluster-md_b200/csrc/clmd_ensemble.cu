@@ -290,18 +290,17 @@ __device__ bool prologue(Rep& R, Cta& C, const Args& A, int step) {
 // cellid[i]), a stable order (by index) of the atoms bucketed by their rows'
 // lengths at the last rebuild.  Per tile of NT atoms, warp ballots rank the
 // atoms of each bucket and the warps' counts (shared memory) place them.
-constexpr int kLenBuckets = 6;
+constexpr int kLenBuckets = 16;  // lengths 0..11 each, 12-14, 15-19, 20-31, 32+
 __device__ __forceinline__ int len_bucket(int len) {
-  return len <= 3 ? 0 : len <= 5 ? 1 : len <= 7 ? 2 : len <= 10 ? 3 : len <= 16 ? 4 : 5;
+  return len <= 11 ? len : len <= 14 ? 12 : len <= 19 ? 13 : len <= 31 ? 14 : 15;
 }
 template <int NT>
 __device__ void length_order(const Rep& R, Cta& C, const Args& A) {
   constexpr int W = NT / 32;
-  static_assert(W * kLenBuckets + kLenBuckets <= (int)(sizeof(C.red) / sizeof(int)),
-                "bucket counts fit the reduction scratch");
+  __shared__ int lsort[W * kLenBuckets + kLenBuckets];
   const int N = R.natom, off = R.off, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const unsigned lt = (1u << lane) - 1u;
-  int* cnt = (int*)C.red;           // [W][kLenBuckets]
+  int* cnt = lsort;                   // [W][kLenBuckets]
   int* base = cnt + W * kLenBuckets;  // [kLenBuckets]
   // bucket sizes -> bucket starts
   int mine[kLenBuckets] = {};
