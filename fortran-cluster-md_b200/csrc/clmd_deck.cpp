@@ -36,20 +36,61 @@ struct Deck {
       if (line[i] != ' ' && line[i] != '\t') out += line[i];
     return out;
   }
-  // Fw.d: without a decimal point the last d digits are the fraction
+  // Fw.d: an optional sign, digits with at most one point, an optional
+  // exponent (E/D/Q with an optional sign, or a bare sign) and digits;
+  // without a point the rightmost d digits are the fraction.  The digits go
+  // to strtod as one decimal string (as gfortran converts them), so the
+  // value is the correctly rounded one.  Any other field stops the
+  // reference's read with a runtime error: here the deck is rejected.
   double F(int skip, int w, int d) {
     next();
-    std::string b = field(skip, w);
+    const std::string b = field(skip, w);
     if (b.empty()) return 0.0;
-    bool point = b.find_first_of(".eEdD") != std::string::npos;
-    for (auto& c : b)
-      if (c == 'd' || c == 'D') c = 'e';
-    double v = strtod(b.c_str(), nullptr);
-    return point ? v : v / pow(10.0, d);
+    size_t k = 0;
+    std::string sign, dig;
+    if (b[k] == '+' || b[k] == '-') sign = b[k++];
+    long point = -1;
+    for (; k < b.size() && ((b[k] >= '0' && b[k] <= '9') || b[k] == '.'); k++) {
+      if (b[k] == '.') {
+        if (point >= 0) return bad();
+        point = (long)dig.size();
+      } else {
+        dig += b[k];
+      }
+    }
+    if (dig.empty() || dig.size() > 120) return bad();
+    long e = 0;
+    if (k < b.size()) {
+      if (strchr("eEdDqQ", b[k])) k++;
+      else if (b[k] != '+' && b[k] != '-') return bad();
+      const bool neg = k < b.size() && b[k] == '-';
+      if (k < b.size() && (b[k] == '+' || b[k] == '-')) k++;
+      if (k == b.size()) return bad();
+      for (; k < b.size(); k++) {
+        if (b[k] < '0' || b[k] > '9') return bad();
+        if (e < 100000) e = 10 * e + (b[k] - '0');
+      }
+      if (neg) e = -e;
+    }
+    if (point < 0) point = (long)dig.size() - d;  // the implied point
+    const std::string s = sign + "0." + dig + "e" + std::to_string(e + point);
+    return strtod(s.c_str(), nullptr);
   }
+  double bad() {
+    ok = false;
+    return 0.0;
+  }
+  // Iw: an optional sign and digits (blanks dropped); anything else is a
+  // runtime error of the reference's read
   int I(int skip) {
     next();
-    std::string b = field(skip, 10);
+    const std::string b = field(skip, 10);
+    size_t k = (!b.empty() && (b[0] == '+' || b[0] == '-')) ? 1 : 0;
+    for (; k < b.size(); k++)
+      if (b[k] < '0' || b[k] > '9') {
+        ok = false;
+        return 0;
+      }
     return b.empty() ? 0 : (int)strtol(b.c_str(), nullptr, 10);
   }
   // (41X,A) into CHARACTER*n: n columns from column 42, blank padded

@@ -24,6 +24,7 @@ struct orc_sys {
   clmd_scalars sc;
   int N;
   int nbmode;
+  int lbmode; /* 0: the reference's O(N^2) labelling loops, 1: union-find */
   /* atomc.inc / atomp.inc, 1-based */
   double *x, *y, *z, *vx, *vy, *vz, *ax, *ay, *az;
   int *api;
@@ -126,6 +127,16 @@ void orc_destroy(orc_sys* S) {
 }
 
 void orc_set_neighbor_mode(orc_sys* S, int mode) { S->nbmode = mode; }
+void orc_set_label_mode(orc_sys* S, int mode) { S->lbmode = mode; }
+
+/* ccf() of the last ten Wolde-Frenkel analysis: 1 for the liquid atoms
+ * (stoddard-pbc-n-m-fre.f:148-168 puts exactly those in liqmon, and the
+ * component sweep :198-225 visits every one of them), 0 otherwise. */
+int orc_get_liquid(orc_sys* S, int32_t* out) {
+  if (!out) return CLMD_ERR_ARG;
+  for (int i = 1; i <= S->N; i++) out[i - 1] = S->ccf[i];
+  return CLMD_OK;
+}
 
 static void cp_in(double* dst1, const double* src0, int N) {
   if (src0) memcpy(dst1 + 1, src0, sizeof(double) * (size_t)N);
@@ -815,6 +826,38 @@ static void bonds_free(bondlists* B) {
   free(B->cvtnt); free(B->cvtn); free(B->cvti); free(B->cvtii); free(B->cvtl);
 }
 
+/* Union-find over the bond lists, restricted to atoms with keep[i] != 0
+ * (NULL: all): lab[i] = the smallest atom number of i's component.  The
+ * reference's sweeps (stoddard-pbc-n-m.f:129-150, -fre.f:171-225) give every
+ * member of a component the counter value of the sweep that found its
+ * smallest member first; label_mode 1 derives the same labels in O(bonds)
+ * so the oracle can check systems too large for the O(N^2) rescans. */
+static int uf_find(int* par, int x) {
+  while (par[x] != x) {
+    par[x] = par[par[x]];
+    x = par[x];
+  }
+  return x;
+}
+static void components(orc_sys* S, const bondlists* B, const int* keep, int* lab) {
+  int N = S->N;
+  int* par = xc((size_t)N + 2, 4);
+  for (int i = 1; i <= N; i++) par[i] = i;
+  for (int i = 1; i <= N; i++) {
+    if (keep && !keep[i]) continue;
+    int ind = B->cvti[i] + 1;
+    for (int k = ind; k <= ind + B->cvtl[i] - 1; k++) {
+      int j = B->cvtn[k];
+      if (keep && !keep[j]) continue;
+      int a = uf_find(par, i), b = uf_find(par, j);
+      if (a == b) continue;
+      if (a < b) par[b] = a; else par[a] = b; /* the root stays the smallest */
+    }
+  }
+  for (int i = 1; i <= N; i++) lab[i] = uf_find(par, i);
+  free(par);
+}
+
 static inline double kin(orc_sys* S, int j) {
   return 0.5 * S->c.apmas[S->api[j] - 1] *
          (S->vx[j] * S->vx[j] + S->vy[j] * S->vy[j] + S->vz[j] * S->vz[j]);
@@ -833,21 +876,33 @@ static int stoddard_stillinger(orc_sys* S, int32_t step) {
   bonds_build(S, 1, &B);
   /* :129-150 */
   int cnum = 0;
-  for (int k = 1; k <= N; k++) {
-    cnum = cnum + 1;
-    int j = k;
-    if (S->cc[j] == 0) {
-    visit:
-      S->cl[j] = cnum;
-      S->cc[j] = 1;
-      S->cs[cnum] = S->cs[cnum] + 1;
-      S->cek[cnum] = S->cek[cnum] + kin(S, j);
-      {
-        int ind = B.cvti[j] + 1;
-        for (int i = ind; i <= ind + B.cvtl[j] - 1; i++) S->cl[B.cvtn[i]] = cnum;
+  if (S->lbmode == 1) {
+    /* the same labels and sizes; cek() summed in atom order, not in the
+     * sweep's visiting order (rounding only) */
+    components(S, &B, NULL, S->cl);
+    for (int i = 1; i <= N; i++) {
+      S->cc[i] = 1;
+      S->cs[S->cl[i]]++;
+      S->cek[S->cl[i]] = S->cek[S->cl[i]] + kin(S, i);
+    }
+    cnum = N;
+  } else {
+    for (int k = 1; k <= N; k++) {
+      cnum = cnum + 1;
+      int j = k;
+      if (S->cc[j] == 0) {
+      visit:
+        S->cl[j] = cnum;
+        S->cc[j] = 1;
+        S->cs[cnum] = S->cs[cnum] + 1;
+        S->cek[cnum] = S->cek[cnum] + kin(S, j);
+        {
+          int ind = B.cvti[j] + 1;
+          for (int i = ind; i <= ind + B.cvtl[j] - 1; i++) S->cl[B.cvtn[i]] = cnum;
+        }
+        for (j = k + 1; j <= N; j++)
+          if (S->cc[j] == 0 && S->cl[j] == cnum) goto visit;
       }
-      for (j = k + 1; j <= N; j++)
-        if (S->cc[j] == 0 && S->cl[j] == cnum) goto visit;
     }
   }
   q->cnum = cnum;
@@ -894,6 +949,54 @@ static int stoddard_frenkel(orc_sys* S, int32_t step) {
         S->cekf[0] = S->cekf[0] + kin(S, k);
       }
     }
+  }
+  if (S->lbmode == 1) {
+    /* :171-195 and :198-225 by union-find.  Liquid components link liquid
+     * atoms only (the sweep never visits a non-liquid atom, so it never
+     * follows that atom's bonds); a liquid component's label is the rank
+     * in liqmon of its smallest member; a non-liquid atom keeps the label
+     * its last liquid neighbour wrote, i.e. the largest of their labels. */
+    components(S, &B, NULL, S->cl);
+    for (int i = 1; i <= N; i++) {
+      S->cc[i] = 1;
+      int r = S->cl[i];
+      if (S->api[i] != 1) {
+        S->cgs[r]++;
+      } else {
+        S->cs[r]++;
+        S->cek[r] = S->cek[r] + kin(S, i);
+      }
+    }
+    cnum = N;
+    int* liq = xc((size_t)N + 2, 4);
+    int* rank = xc((size_t)N + 2, 4);
+    for (int k = 1; k <= nliqmon; k++) {
+      liq[liqmon[k]] = 1;
+      rank[liqmon[k]] = k;
+    }
+    int* lab = xc((size_t)N + 2, 4);
+    components(S, &B, liq, lab);
+    for (int k = 1; k <= nliqmon; k++) {
+      int m = liqmon[k];
+      int f = rank[lab[m]];
+      S->clf[m] = f;
+      S->ccf[m] = 1;
+      S->csf[f]++;
+      S->cekf[f] = S->cekf[f] + kin(S, m);
+    }
+    for (int i = 1; i <= N; i++) {
+      if (liq[i]) continue;
+      int ind = B.cvti[i] + 1, f = 0;
+      for (int k = ind; k <= ind + B.cvtl[i] - 1; k++)
+        if (liq[B.cvtn[k]] && S->clf[B.cvtn[k]] > f) f = S->clf[B.cvtn[k]];
+      S->clf[i] = f;
+    }
+    free(lab);
+    free(rank);
+    free(liq);
+    q->cnum = cnum;
+    q->cnumf = nliqmon;
+    goto tally;
   }
   /* :171-195 */
   for (int k = 1; k <= N; k++) {
@@ -945,7 +1048,9 @@ static int stoddard_frenkel(orc_sys* S, int32_t step) {
   }
   q->cnum = cnum;
   q->cnumf = cnumf;
+tally:;
   /* :229-241 */
+  cnumf = q->cnumf;
   int maxcs = 0;
   for (int i = 1; i <= cnum; i++) {
     if (S->cs[i] > q->cbiggest) q->cbiggest = S->cs[i];
@@ -1186,23 +1291,82 @@ static void dk_field(deck* d, int skip, int w, char* out) {
     if (d->line[i] != ' ' && d->line[i] != '\t') out[k++] = d->line[i];
   out[k] = 0;
 }
-/* Fw.d input: without a decimal point the last d digits are the fraction */
+/* What gfortran's formatted input accepts (blanks already dropped, BN):
+ * Iw an optional sign and digits; Fw.d an optional sign, digits with at
+ * most one point, and an exponent (a letter E/D/Q with an optional sign, or
+ * a bare sign) followed by digits.  Anything else stops the reference's
+ * read with a runtime error ("Bad value during ... read"). */
+static int dk_int_ok(const char* b) {
+  if (*b == '+' || *b == '-') b++;
+  for (; *b; b++)
+    if (*b < '0' || *b > '9') return 0;
+  return 1;
+}
+/* Fw.d of a blank-free field b: 1 and *v on success, 0 where gfortran
+ * stops the read.  Without a decimal point the rightmost d digits of the
+ * mantissa are the fraction (an exponent, if any, scales the result); the
+ * digits are handed to strtod as one decimal string, as gfortran does, so
+ * the value is the correctly rounded one. */
+static int dk_real(const char* b, int d, double* v) {
+  char m[160];
+  int k = 0, nd = 0, point = -1;
+  if (*b == '+' || *b == '-') m[k++] = *b++;
+  const int m0 = k;
+  for (; (*b >= '0' && *b <= '9') || *b == '.'; b++) {
+    if (*b == '.') {
+      if (point >= 0) return 0;
+      point = nd;
+      continue;
+    }
+    if (k > 120) return 0;
+    m[k++] = *b;
+    nd++;
+  }
+  if (!nd) return 0;
+  long e = 0;
+  if (*b) {
+    if (strchr("eEdDqQ", *b)) b++;
+    else if (*b != '+' && *b != '-') return 0;
+    int neg = *b == '-';
+    if (*b == '+' || *b == '-') b++;
+    if (!*b) return 0;
+    for (; *b; b++) {
+      if (*b < '0' || *b > '9') return 0;
+      if (e < 100000) e = 10 * e + (*b - '0');
+    }
+    if (neg) e = -e;
+  }
+  if (point < 0) point = nd - d;  /* the implied point */
+  /* digits d1..dn with the point after `point` digits: 0.d1..dn x 10^point */
+  char out[200];
+  int o = 0;
+  if (m0) out[o++] = m[0];
+  out[o++] = '0';
+  out[o++] = '.';
+  for (int i = m0; i < k; i++) out[o++] = m[i];
+  o += snprintf(out + o, sizeof out - o, "e%ld", e + point);
+  *v = strtod(out, NULL);
+  return 1;
+}
+
+/* Fw.d input (see dk_real) */
 static double dk_f(deck* d, int skip, int w, int dd) {
   char b[128];
   dk_next(d);
   dk_field(d, skip, w, b);
   if (!b[0]) return 0.0;
-  if (strchr(b, '.') || strchr(b, 'e') || strchr(b, 'E') || strchr(b, 'd') || strchr(b, 'D')) {
-    for (char* p = b; *p; p++)
-      if (*p == 'd' || *p == 'D') *p = 'e';
-    return strtod(b, NULL);
-  }
-  return strtod(b, NULL) / pow(10.0, dd);
+  double v = 0.0;
+  if (!dk_real(b, dd, &v)) d->ok = 0;
+  return v;
 }
 static int dk_i(deck* d, int skip) {
   char b[128];
   dk_next(d);
   dk_field(d, skip, 10, b);
+  if (!dk_int_ok(b)) {
+    d->ok = 0;
+    return 0;
+  }
   return b[0] ? (int)strtol(b, NULL, 10) : 0;
 }
 static char dk_a1(deck* d) {
@@ -1315,4 +1479,182 @@ int orc_readdata(const char* path, clmd_config* cfg, int32_t* ntim, int32_t* sct
   if (sctim) *sctim = sc;
   fclose(d.f);
   return d.ok ? 0 : 3;
+}
+
+/* ------------------------------------------------------------------------ */
+/* The engine's seeded start configuration, restated so that the CPU        */
+/* baseline can build its inputs without loading the engine library: the    */
+/* same xoshiro256** stream (seeded by splitmix64), the same rejection of    */
+/* pairs nearer than rmin on a cell grid, the same Box-Muller velocities.    */
+/* It must give the engine's clmd_init_random() bytes exactly (tested).      */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  uint64_t s[4];
+} orc_rng;
+
+static uint64_t orc_splitmix(uint64_t* x) {
+  uint64_t z = (*x += 0x9e3779b97f4a7c15ull);
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+static uint64_t orc_rotl(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+static uint64_t orc_next(orc_rng* r) {
+  uint64_t* s = r->s;
+  uint64_t res = orc_rotl(s[1] * 5, 7) * 9, t = s[1] << 17;
+  s[2] ^= s[0];
+  s[3] ^= s[1];
+  s[1] ^= s[2];
+  s[0] ^= s[3];
+  s[2] ^= t;
+  s[3] = orc_rotl(s[3], 45);
+  return res;
+}
+static double orc_uniform(orc_rng* r) {
+  return (double)(orc_next(r) >> 11) * (1.0 / 9007199254740992.0);
+}
+static double orc_gauss(orc_rng* r) {
+  double u1 = orc_uniform(r), u2 = orc_uniform(r);
+  if (u1 < 1e-300) u1 = 1e-300;
+  return sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+}
+
+int orc_init_random(int32_t n, double bx, double by, double bz, double rmin, double kT_over_m,
+                    uint64_t seed, double* x, double* y, double* z, double* vx, double* vy,
+                    double* vz) {
+  if (n < 1 || !(bx > 0 && by > 0 && bz > 0) || rmin < 0 || !x || !y || !z)
+    return CLMD_ERR_ARG;
+  orc_rng rng;
+  for (int i = 0; i < 4; i++) rng.s[i] = orc_splitmix(&seed);
+  double vol = bx * by * bz;
+  double side = cbrt(vol / n);
+  if (side < rmin) side = rmin;
+  int nx = (int)(bx / side), ny = (int)(by / side), nz = (int)(bz / side);
+  if (nx < 1) nx = 1;
+  if (ny < 1) ny = 1;
+  if (nz < 1) nz = 1;
+  int* head = xc((size_t)nx * ny * nz, 4);
+  int* next = xc((size_t)n, 4);
+  for (size_t k = 0; k < (size_t)nx * ny * nz; k++) head[k] = -1;
+  for (int i = 0; i < n; i++) next[i] = -1;
+  double r2 = rmin * rmin;
+  int rc = CLMD_OK;
+  for (int i = 0; i < n && rc == CLMD_OK; i++) {
+    int tries = 0;
+    for (;;) {
+      if (++tries > 100000) {
+        rc = CLMD_ERR_ARG;
+        break;
+      }
+      double px = orc_uniform(&rng) * bx, py = orc_uniform(&rng) * by,
+             pz = orc_uniform(&rng) * bz;
+      int c0 = (int)(px / bx * nx), c1 = (int)(py / by * ny), c2 = (int)(pz / bz * nz);
+      if (c0 > nx - 1) c0 = nx - 1;
+      if (c1 > ny - 1) c1 = ny - 1;
+      if (c2 > nz - 1) c2 = nz - 1;
+      int ok = 1;
+      for (int a = -1; a <= 1 && ok; a++)
+        for (int b = -1; b <= 1 && ok; b++)
+          for (int d = -1; d <= 1 && ok; d++) {
+            int xx = (c0 + d + nx) % nx, yy = (c1 + b + ny) % ny, zz = (c2 + a + nz) % nz;
+            for (int j = head[((size_t)zz * ny + yy) * nx + xx]; j >= 0; j = next[j]) {
+              double dx = px - x[j], dy = py - y[j], dz = pz - z[j];
+              dx -= bx * nearbyint(dx / bx);
+              dy -= by * nearbyint(dy / by);
+              dz -= bz * nearbyint(dz / bz);
+              if (dx * dx + dy * dy + dz * dz < r2) {
+                ok = 0;
+                break;
+              }
+            }
+          }
+      if (!ok) continue;
+      x[i] = px;
+      y[i] = py;
+      z[i] = pz;
+      size_t k = ((size_t)c2 * ny + c1) * nx + c0;
+      next[i] = head[k];
+      head[k] = i;
+      break;
+    }
+  }
+  free(head);
+  free(next);
+  if (rc) return rc;
+  double sd = sqrt(kT_over_m > 0 ? kT_over_m : 0.0);
+  for (int i = 0; i < n; i++) {
+    double a = orc_gauss(&rng), b = orc_gauss(&rng), c = orc_gauss(&rng);
+    if (vx) vx[i] = sd * a;
+    if (vy) vy[i] = sd * b;
+    if (vz) vz[i] = sd * c;
+  }
+  return CLMD_OK;
+}
+
+/* ------------------------------------------------------------------------ */
+/* helpers/passage-time.f:47-90 on one run's analysis record: ts[k] the     */
+/* step and cs[k] the largest cluster size of analysis k (the columns the   */
+/* reference reads from its sizer file).  pt[j] (j = 0..endsize) receives   */
+/* the first step at which the largest cluster reached size j for j >=     */
+/* startsize (-1 where it never did; the lines the reference writes to its  */
+/* dump), probab[j] the reference's probab.largest counts: analyses at or   */
+/* after `warmup` with largest size j, up to and including the one that     */
+/* first reached endsize.  Returns the next size not reached (the           */
+/* reference's i at :77).                                                   */
+/* ------------------------------------------------------------------------ */
+int orc_passage_time(const int32_t* ts, const int32_t* cs, int32_t nlines, int32_t startsize,
+                     int32_t endsize, int32_t warmup, int32_t* pt, int32_t* probab) {
+  for (int j = 0; j <= endsize; j++) {
+    if (pt) pt[j] = -1;
+    if (probab) probab[j] = 0;
+  }
+  int i = startsize, flag = -1;
+  for (int k = 0; k < nlines; k++) {
+    const int t = ts[k], c = cs[k];
+    /* :62-65 */
+    if (flag != 1) {
+      if (c >= endsize) flag = 1;
+      if (t >= warmup && probab && c >= 0 && c <= endsize) probab[c] = probab[c] + 1;
+    }
+    /* :67-72 */
+    if (c >= i) {
+      for (int j = i; j <= c; j++)
+        if (pt && j <= endsize) pt[j] = t;
+      i = c + 1;
+    }
+  }
+  return i;
+}
+
+/* helpers/mpt.f:52-110 over the pooled dump lines of many runs (size cs[k]
+ * first reached at step ts[k]): for every size i in startsize..endsize,
+ * mpt[i - startsize] = mean of ts/500000 (the reference's nanoseconds at a
+ * 2 fs step, :80), stda = sqrt((mean of squares - mean^2) / count) (:95-97)
+ * and count.  A size no run reached gives 0/0 as in the reference (NaN). */
+int orc_mpt(const int32_t* ts, const int32_t* cs, int32_t nlines, int32_t startsize,
+            int32_t endsize, double* mpt, double* stda, int32_t* count) {
+  if (startsize < 1 || endsize > 4096 || endsize < startsize) return CLMD_ERR_ARG;
+  double pt[4097], ptsq[4097];
+  int cnt[4097];
+  for (int i = 0; i <= 4096; i++) {
+    pt[i] = 0.0;
+    ptsq[i] = 0.0;
+    cnt[i] = 0;
+  }
+  for (int k = 0; k < nlines; k++) {
+    const int c = cs[k];
+    if (c < 1 || c > 4096) continue;
+    pt[c] = pt[c] + (double)ts[k] / 500000;
+    ptsq[c] = ptsq[c] + ((double)ts[k] / 500000) * ((double)ts[k] / 500000);
+    cnt[c] = cnt[c] + 1;
+  }
+  for (int i = startsize; i <= endsize; i++) {
+    const double m = pt[i] / cnt[i];
+    double sd = ptsq[i] / cnt[i] - m * m;
+    sd = sqrt(sd / cnt[i]);
+    mpt[i - startsize] = m;
+    stda[i - startsize] = sd;
+    count[i - startsize] = cnt[i];
+  }
+  return CLMD_OK;
 }

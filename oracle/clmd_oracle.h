@@ -29,6 +29,13 @@ void orc_destroy(orc_sys* S);
  * 1 = cell list that must yield the same list (used for large N). */
 void orc_set_neighbor_mode(orc_sys* S, int mode);
 
+/* 0 = the reference's labelling sweeps, O(N^2) per analysis (default),
+ * 1 = union-find giving the same labels, sizes and histograms (cluster
+ * energies summed in atom order), for systems too large for the sweeps. */
+void orc_set_label_mode(orc_sys* S, int mode);
+/* 1 for the atoms the last ten Wolde-Frenkel analysis found liquid. */
+int orc_get_liquid(orc_sys* S, int32_t* out);
+
 void orc_scalars_init(const clmd_config* cfg, clmd_scalars* sc);
 
 void orc_set_state(orc_sys* S, const double* x, const double* y, const double* z,
@@ -67,6 +74,26 @@ int64_t orc_neighbor_rows_sample(orc_sys* S, int32_t i0, int32_t i1);
 /* Reads a .3d deck like read-3d.f:11-302 into cfg (+ the file interval
  * ftcsi, ntim, sctim).  Returns 0 on success. */
 int orc_readdata(const char* path, clmd_config* cfg, int32_t* ntim, int32_t* sctim);
+
+/* The engine's seeded start (uniform positions no pair nearer than rmin,
+ * Maxwell-Boltzmann velocities), restated so a CPU-only process can build
+ * the same inputs without the engine library.  Byte-identical to
+ * clmd_init_random(). */
+int orc_init_random(int32_t n, double bx, double by, double bz, double rmin, double kT_over_m,
+                    uint64_t seed, double* x, double* y, double* z, double* vx, double* vy,
+                    double* vz);
+
+/* helpers/passage-time.f:47-90 on one run's (step, largest cluster size)
+ * analysis record: pt[0..endsize] first step each size >= startsize was
+ * reached (-1 never), probab[0..endsize] the probab.largest counts; returns
+ * the first size not reached. */
+int orc_passage_time(const int32_t* ts, const int32_t* cs, int32_t nlines, int32_t startsize,
+                     int32_t endsize, int32_t warmup, int32_t* pt, int32_t* probab);
+/* helpers/mpt.f:52-110 over pooled passage-time lines (size cs[k] first
+ * reached at step ts[k]): per size startsize..endsize the mean of
+ * ts/500000, its standard error and the count. */
+int orc_mpt(const int32_t* ts, const int32_t* cs, int32_t nlines, int32_t startsize,
+            int32_t endsize, double* mpt, double* stda, int32_t* count);
 
 #ifdef __cplusplus
 }

@@ -63,6 +63,13 @@ def load():
         "orc_get_clusters": ([P, C.POINTER(clmd.ClusterView)], C.c_int),
         "orc_neighbor_rows_sample": ([P, C.c_int32, C.c_int32], C.c_int64),
         "orc_readdata": ([C.c_char_p, C.POINTER(clmd.Config), i, i], C.c_int),
+        "orc_set_label_mode": ([P, C.c_int], None),
+        "orc_get_liquid": ([P, i], C.c_int),
+        "orc_init_random": ([C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double,
+                             C.c_double, C.c_uint64, d, d, d, d, d, d], C.c_int),
+        "orc_passage_time": ([i, i, C.c_int32, C.c_int32, C.c_int32, C.c_int32, i, i],
+                             C.c_int),
+        "orc_mpt": ([i, i, C.c_int32, C.c_int32, C.c_int32, d, d, i], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -82,6 +89,45 @@ def scalars_init(cfg):
     return s
 
 
+def init_random(n, box, rmin, kt_over_m, seed):
+    """The engine's seeded start, computed here without the engine library
+    (byte-identical to clmd.init_random)."""
+    arrs = [np.zeros(n) for _ in range(6)]
+    bx, by, bz = box
+    st = load().orc_init_random(n, bx, by, bz, rmin, kt_over_m, seed,
+                                *[ptr(a, C.c_double) for a in arrs])
+    if st:
+        raise RuntimeError(f"orc_init_random failed: {st}")
+    return tuple(arrs)
+
+
+def passage_time(ts, cs, startsize, endsize, warmup=0):
+    """helpers/passage-time.f on one run: (first-passage step per size
+    0..endsize, -1 where never reached; probab.largest counts)."""
+    ts = np.ascontiguousarray(ts, dtype=np.int32)
+    cs = np.ascontiguousarray(cs, dtype=np.int32)
+    pt = np.zeros(endsize + 1, dtype=np.int32)
+    pb = np.zeros(endsize + 1, dtype=np.int32)
+    load().orc_passage_time(ptr(ts, C.c_int32), ptr(cs, C.c_int32), len(ts), startsize,
+                            endsize, warmup, ptr(pt, C.c_int32), ptr(pb, C.c_int32))
+    return pt, pb
+
+
+def mpt(ts, cs, startsize, endsize):
+    """helpers/mpt.f over pooled (step, size) passage lines: per size
+    startsize..endsize (mean of ts/500000, standard error, count)."""
+    ts = np.ascontiguousarray(ts, dtype=np.int32)
+    cs = np.ascontiguousarray(cs, dtype=np.int32)
+    n = endsize - startsize + 1
+    m, sd = np.zeros(n), np.zeros(n)
+    cnt = np.zeros(n, dtype=np.int32)
+    st = load().orc_mpt(ptr(ts, C.c_int32), ptr(cs, C.c_int32), len(ts), startsize, endsize,
+                        ptr(m, C.c_double), ptr(sd, C.c_double), ptr(cnt, C.c_int32))
+    if st:
+        raise RuntimeError(f"orc_mpt failed: {st}")
+    return m, sd, cnt
+
+
 def readdata(path):
     cfg = clmd.Config()
     nt = C.c_int32(0)
@@ -93,12 +139,13 @@ def readdata(path):
 
 
 class Oracle:
-    def __init__(self, cfg, neighbor_mode=0):
+    def __init__(self, cfg, neighbor_mode=0, label_mode=0):
         self.lib = load()
         self.cfg = cfg
         self.n = cfg.natom
         self.h = self.lib.orc_create(C.byref(cfg))
         self.lib.orc_set_neighbor_mode(self.h, neighbor_mode)
+        self.lib.orc_set_label_mode(self.h, label_mode)
 
     def close(self):
         if self.h:
@@ -198,6 +245,12 @@ class Oracle:
             out[name] = a
             setattr(v, name, ptr(a, C.c_int32 if dt == np.int32 else C.c_double))
         self.lib.orc_get_clusters(self.h, C.byref(v))
+        return out
+
+    def liquid(self):
+        """1 for the atoms the last ten Wolde-Frenkel analysis found liquid."""
+        out = np.zeros(self.n, dtype=np.int32)
+        self.lib.orc_get_liquid(self.h, ptr(out, C.c_int32))
         return out
 
     def neighbor_rows_sample(self, i0, i1):

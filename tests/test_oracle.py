@@ -249,3 +249,79 @@ def test_oracle_rates_warning_and_quiet_step(tmp_path):
     assert not out.exists()
     assert o.rates(6, 1, str(out), str(log)) == 0  # same positions: same clusters
     assert not out.exists()
+
+
+@pytest.mark.parametrize("clustering", [clmd.CLU_STILLINGER, clmd.CLU_FRENKEL])
+@pytest.mark.parametrize("n,rho,two", [(3000, 0.3, False), (6000, 0.12, False),
+                                       (5000, 0.18, True), (8000, 0.2, False)])
+def test_union_find_labels_equal_reference_sweeps(clustering, n, rho, two):
+    """label_mode 1 (union-find, O(bonds)) gives the reference sweeps'
+    labels, sizes, histograms, liquid atoms, counters and first-passage
+    stamps bit for bit (cluster energies to rounding): the checker for the
+    systems too large for the O(N^2) sweeps.  Two analyses in a row, so the
+    never-reset csi(0) and the running cbiggest/clookfor take part."""
+    sp = dict(n=n // 5, sigma=0.758, eps=0.085, mass=0.1) if two else None
+    cfg = clmd.lj_config(n, rho, 0.7, clustering=clustering, atnenum=3, species=sp)
+    st = random_state(cfg, 5)
+    out = []
+    for mode in (0, 1):
+        o = orc.Oracle(cfg, neighbor_mode=1, label_mode=mode)
+        o.set_state(st, scalars=orc.scalars_init(cfg))
+        o.neighbor(0)
+        o.stoddard(3)
+        o.stoddard(4)
+        out.append((o.clusters(), o.scalars(), o.liquid()))
+        o.close()
+    (ca, sa, la), (cb, sb, lb) = out
+    for k in ca:
+        if ca[k].dtype == np.int32:
+            assert np.array_equal(ca[k], cb[k]), k
+        else:
+            np.testing.assert_allclose(ca[k], cb[k], rtol=1e-12, atol=1e-12, err_msg=k)
+    assert np.array_equal(la, lb)
+    if clustering == clmd.CLU_FRENKEL:
+        assert la.sum() > 0
+    for f in ("cnum", "cnumf", "cbiggest", "cbiggestf", "clookfor", "clookforf", "maxcs"):
+        assert getattr(sa, f) == getattr(sb, f), f
+
+
+def test_init_random_restatement_is_byte_identical():
+    """The oracle's copy of the seeded start gives the engine's bytes, so a
+    CPU-only process builds the same inputs without the engine library."""
+    for n, rho, seed in [(1000, 0.01, 3), (5000, 0.3, 9), (200, 0.05, 1)]:
+        L = (n / rho) ** (1.0 / 3.0)
+        a = clmd.init_random(n, (L, L, L), 0.9, 0.7, seed)
+        b = orc.init_random(n, (L, L, L), 0.9, 0.7, seed)
+        for u, v in zip(a, b):
+            assert np.array_equal(u, v)
+
+
+def test_passage_time_known_answers():
+    """helpers/passage-time.f:47-90 on a hand-made sizer record: sizes are
+    stamped with the first analysis whose largest cluster reaches them; a
+    jump stamps every size in between; a shrinking cluster stamps nothing;
+    probab.largest counts analyses from `warmup` until (and including) the
+    one that first reaches endsize."""
+    ts = [0, 100, 200, 300, 400, 500, 600]
+    cs = [1, 3, 2, 6, 5, 9, 12]
+    pt, pb = orc.passage_time(ts, cs, startsize=2, endsize=8, warmup=100)
+    assert pt.tolist() == [-1, -1, 100, 100, 300, 300, 300, 500, 500]
+    # counted: 100(3), 200(2), 300(6), 400(5), 500(9 >= endsize: counted, then stop)
+    assert pb.tolist() == [0, 0, 1, 1, 0, 1, 1, 0, 0]
+    pt, _ = orc.passage_time(ts, cs, startsize=1, endsize=12)
+    assert pt.tolist() == [-1, 0, 100, 100, 300, 300, 300, 500, 500, 500, 600, 600, 600]
+
+
+def test_mpt_known_answers():
+    """helpers/mpt.f:52-110: per size the mean of ts/500000 (nanoseconds at
+    a 2 fs step), the standard error sqrt((<t^2> - <t>^2) / count), the
+    count; an unreached size is 0/0 as in the reference."""
+    ts = [500000, 1500000, 1000000, 250000]
+    cs = [3, 3, 4, 3]
+    m, sd, cnt = orc.mpt(ts, cs, 3, 5)
+    assert cnt.tolist() == [3, 1, 0]
+    t3 = np.array([1.0, 3.0, 0.5])
+    assert m[0] == pytest.approx(t3.mean(), rel=1e-15)
+    assert sd[0] == pytest.approx(math.sqrt(((t3 ** 2).mean() - t3.mean() ** 2) / 3), rel=1e-12)
+    assert m[1] == 2.0 and sd[1] == 0.0
+    assert math.isnan(m[2]) and math.isnan(sd[2])
