@@ -365,6 +365,7 @@ __global__ void k_clear_status(DevState* st) {
   st->s.fail_step = 0;
   st->s.aborted = 0;
   st->err_new = 0;
+  st->bar_count = 0;  // a barrier that timed out leaves its arrivals counted
 }
 
 __global__ void k_merge_err(DevState* st) {
@@ -373,6 +374,22 @@ __global__ void k_merge_err(DevState* st) {
     st->s.status = err;
     st->s.fail_step = st->cur_step;
   }
+}
+
+__global__ void k_debug_barrier(DevState* st, unsigned int extra, long long limit) {
+  st->bar_extra = extra;
+  st->bar_limit = limit;
+  st->bar_count = 0;
+}
+
+extern "C" int clmd_debug_barrier(clmd_system* S, int32_t extra_arrivals, int64_t spin_limit) {
+  if (!S || extra_arrivals < 0 || spin_limit < 0) return set_last(CLMD_ERR_ARG);
+  CK(cudaStreamSynchronize(S->stream));
+  k_debug_barrier<<<1, 1, 0, S->stream>>>(S->st, (unsigned)extra_arrivals, (long long)spin_limit);
+  S->launches++;
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(S->stream));
+  return set_last(CLMD_OK);
 }
 
 extern "C" int clmd_clear_status(clmd_system* S) {

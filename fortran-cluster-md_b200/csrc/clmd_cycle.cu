@@ -67,16 +67,20 @@ __device__ __forceinline__ bool gbar(DevState* st) {
     __threadfence();
     unsigned int arrived = atomicAdd(&st->bar_count, 1u);
     fail = 0;
-    if (arrived == gridDim.x - 1) {
+    if (arrived == gridDim.x - 1 + st->bar_extra) {
       atomicExch(&st->bar_count, 0u);
       __threadfence();
       atomicAdd(&st->bar_gen, 1u);
     } else {
+      const long long limit = st->bar_limit > 0 ? st->bar_limit : (1ll << 25);
       long long spins = 0;
       while (*gen == g) {
         __nanosleep(32);
-        if (++spins > (1ll << 25)) {
+        if (++spins > limit) {
           fail = 1;
+          // recorded here as well: a rebuild cut short by a timeout leaves
+          // the launch through its normal end, which latches err_new
+          atomicCAS(&st->err_new, 0, CLMD_ERR_TIMEOUT);
           break;
         }
       }

@@ -73,6 +73,10 @@ struct DevState {
   int clu_force;                // next analysis runs even if cstep == step
   unsigned int ctr[16];         // last-block counters (one per reduction site)
   unsigned int bar_count, bar_gen;  // grid barrier of cooperative kernels
+  // failure-path tests only (clmd_debug_barrier): arrivals a barrier waits
+  // for beyond the grid (0 in use), and its spin limit (0: the default)
+  unsigned int bar_extra, bar_pad;
+  long long bar_limit;
 };
 
 enum CtrSlot {

@@ -17,36 +17,26 @@
 // start at zero; it keeps the last call's contents.
 #include <cuda_runtime.h>
 
-#include <mutex>
-
 #include "../../include/clmd.h"
 
 static __device__ __align__(256) int g_noalloc_parent[CLMD_NOALLOC_MAX_ATOMS];
 
 namespace {
 
-constexpr int kMaxDevices = 64;
-int* g_parent_addr[kMaxDevices];  // device address of g_noalloc_parent, per device
-std::mutex g_setup_mutex;
-
 // Host code cannot use g_noalloc_parent as a device address (it names a
-// host-side stand-in); ask the runtime once per device, with that device
-// current.
+// host-side stand-in): ask the runtime for the address on the current device
+// at every call.  The lookup is cheap once the module is loaded, and a
+// cached value could outlive the context it came from (after
+// cudaDeviceReset the module may load at another address).  The first call
+// on a device loads the module; make it before any stream capture.
 int parent_address(int** out) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return CLMD_ERR_CUDA;
-  if (dev < 0 || dev >= kMaxDevices) return CLMD_ERR_ARG;
-  std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_parent_addr[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_parent);
-    if (e != cudaSuccess || !p) {
-      cudaGetLastError();
-      return CLMD_ERR_CUDA;
-    }
-    g_parent_addr[dev] = (int*)p;
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_parent);
+  if (e != cudaSuccess || !p) {
+    cudaGetLastError();  // the lookup's own error, raised just now
+    return CLMD_ERR_CUDA;
   }
-  *out = g_parent_addr[dev];
+  *out = (int*)p;
   return CLMD_OK;
 }
 
@@ -151,6 +141,9 @@ extern "C" int clmd_stoddard_noalloc(int32_t natom, const double* x, const doubl
   if (!x || !y || !z || !api || !atnlist || !atnidx || !cl || !cs || !csi || nlist < natom)
     return CLMD_ERR_ARG;
   if (!(boxx > 0 && boxy > 0 && boxz > 0 && sigma1 > 0)) return CLMD_ERR_ARG;
+  // an error left by the caller's earlier work stays the caller's: report
+  // it without launching and without clearing it
+  if (cudaPeekAtLastError() != cudaSuccess) return CLMD_ERR_CUDA;
   int* par = nullptr;
   int st = parent_address(&par);
   if (st) return st;
@@ -165,5 +158,6 @@ extern "C" int clmd_stoddard_noalloc(int32_t natom, const double* x, const doubl
                                       boxz, bf1, bf2, rc2, par);
   k_na_label<<<nb, kThreads, 0, s>>>(natom, par, cl, cs);
   k_na_hist<<<nb, kThreads, 0, s>>>(natom, cs, csi);
+  // the error state was clean on entry: anything pending now is these launches'
   return cudaGetLastError() == cudaSuccess ? CLMD_OK : CLMD_ERR_CUDA;
 }

@@ -439,15 +439,25 @@ int clmd_serve(clmd_ensemble* e, const clmd_request* reqs, int32_t nreq, double 
  * entries) and atnidx, and the outputs cl[natom], cs[natom],
  * csi[natom+1] (csi[0] accumulates across calls like the reference's).
  * Enqueued on `stream`; natom > CLMD_NOALLOC_MAX_ATOMS returns CLMD_ERR_ARG.
- * The first call on each device looks up the array's device address (make
- * it before any stream capture).  Every call shares the array, so calls that
- * overlap on the GPU race: serialise them. */
+ * Every call looks up the array's address on the current device; the first
+ * call on a device loads the module (make it before any stream capture).  A
+ * CUDA error left pending by the caller's earlier work is reported as
+ * CLMD_ERR_CUDA, without launching and without clearing it.  Every call
+ * shares the array, so calls that overlap on the GPU race: serialise them. */
 #define CLMD_NOALLOC_MAX_ATOMS (1 << 20)
 int clmd_stoddard_noalloc(int32_t natom, const double* x, const double* y, const double* z,
                           const int32_t* api, const int32_t* atnlist, int64_t nlist,
                           const int32_t* atnidx, double boxx, double boxy, double boxz,
                           double atrskin, double sigma1, double atskin, int32_t* cl,
                           int32_t* cs, int32_t* csi, void* stream);
+
+/* Failure-path testing of the grid barrier of the persistent kernels: from
+ * now on every barrier of this system waits for `extra_arrivals` blocks
+ * beyond the grid (none come) and gives up after `spin_limit` polls (0: the
+ * default, ~2 s); the launch then ends with CLMD_ERR_TIMEOUT, latched in the
+ * status like any other error.  (0, 0) restores normal barriers.  Only for
+ * tests: a timed-out system must be cleared (clmd_clear_status) or dropped. */
+int clmd_debug_barrier(clmd_system* S, int32_t extra_arrivals, int64_t spin_limit);
 
 const char* clmd_status_string(int status);
 /* sizeof of the ABI structs (0 config, 1 scalars, 2 cluster view, 3 ensemble

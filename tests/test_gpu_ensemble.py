@@ -387,6 +387,53 @@ def test_mean_first_passage_matches_per_replica_tables(gpu):
     assert cnt[0] == len(slots) and cnt[4] > 0  # every replica has monomers; some dimers+
 
 
+def test_first_passage_follows_reference_helpers(gpu):
+    """Each replica's first-passage table is helpers/passage-time.f:55-75
+    (the oracle's restatement) applied to that replica's record of
+    (analysis step, largest cluster size), polled window by window; pooled
+    over the replicas, clmd_ens_mfpt is helpers/mpt.f:73-110 with the
+    reference's ts/500000 scaling (nanoseconds at a 2 fs step), the same
+    counts and standard errors."""
+    rng = np.random.default_rng(33)
+    win = 25
+    e = clmd.Ensemble(clmd.ens_config(40 * 1500, 40, ftcsi=win, threads=256))
+    slots = []
+    for k in range(40):
+        n = int(rng.integers(300, 1500))
+        box, arrs = replica_inputs(n, float(rng.uniform(0.03, 0.05)), 0.65, 900 + k)
+        slots.append(e.add(n, box, 0.65, *arrs, csover=10**6, budget=0))
+    rec = {s: ([], []) for s in slots}
+    for w in range(1, 25):
+        e.step(1)
+        res = e.results()
+        for s in slots:
+            assert res[s].step == win * w and res[s].status == 0
+            rec[s][0].append(win * (w - 1))  # the analysis opens each window
+            rec[s][1].append(res[s].maxcs)
+    cap = 128
+    pool_ts, pool_cs = [], []
+    for s in slots:
+        pt, _ = orc.passage_time(rec[s][0], rec[s][1], 1, cap)
+        assert np.array_equal(e.fpt(s, cap), pt[1:]), s
+        for j in range(1, cap + 1):
+            if pt[j] >= 0:
+                pool_ts.append(pt[j])
+                pool_cs.append(j)
+    m, sd, cnt = orc.mpt(pool_ts, pool_cs, 1, cap)
+    mean, sem, ecnt = e.mfpt(cap)
+    assert np.array_equal(ecnt, cnt)
+    for j in range(cap):
+        if cnt[j] == 0:
+            assert mean[j] == -1.0
+            continue
+        np.testing.assert_allclose(mean[j] / 500000, m[j], rtol=1e-12)
+        if np.isnan(sd[j]):  # all passages at one step: mpt.f's sqrt of a rounding residue
+            assert sem[j] <= 1e-6 * mean[j]
+        else:
+            assert abs(sem[j] / 500000 - sd[j]) <= 1e-12 * m[j] + 1e-9 * sd[j]
+    assert cnt[0] == len(slots) and cnt[3] > 0
+
+
 def test_graph_replay_same_as_direct_launches(gpu, monkeypatch):
     """The window sequence replayed from a CUDA graph (default) and issued
     launch by launch (CLMD_ENS_GRAPHS=0) give bit-identical replicas, also
