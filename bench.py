@@ -21,11 +21,22 @@ A bench step is one window: every running replica advances 100 steps
   roofline  the window kernels (k_ens, 4 size classes concurrently), CUDA
           events inside the library; 120 algorithmic bytes per atom-step
           (x, v FP64 and a FP32, read + written) against measured HBM.
+  fp64_ensemble_same_ensemble  the same replicas as an all-FP64 ensemble
+          (same kernels, FP64 pair terms and sums).
   fp64_dropin_same_ensemble  the FP64 drop-in (one system at a time, the
           plain engine) timed on replicas at the size quantiles, summed over
           the whole ensemble: the "vs FP64" of the metric.
-  cpu_baseline  the serial C restatement of the reference on one core,
-          sampled on replicas at the size quantiles.
+  mixed_vs_fp64_sample  64 replicas run mixed, FP64 and as an FP64 twin
+          (1e-13 apart) for 1e4 steps: per-replica energy drift, mixed - FP64
+          against the twin's spread, the drift of the energy the truncated
+          force conserves, the cluster-size distribution.
+  served  configs[4] on the same GPU: a bounded Poisson window at 200
+          requests/s served with continuous batching; p50/p99 request
+          latency (censored requests at their lower bound), time to
+          nucleation (wall and step), aggregate atom-steps/s.
+  cpu_baseline  the serial C restatement of the reference (the oracle) on
+          one pinned core, on 16 replicas at the midpoints of 16 size strata,
+          3 timed 100-step windows: the rate of exactly that timed work.
 
 --workload dropin: one FP64 system of N = 262,144 atoms (rho* = 0.02, T* =
 0.7, velocity Verlet, Stillinger every 100 steps), a bench step = one
@@ -35,12 +46,14 @@ analysis cycle of 100 steps.
 0.05, T* = 0.75, Nose-Hoover with Q = N T* 0.25, FP32 pair terms with Kahan
 FP32 sums, FP64 positions, velocities, PSI and energies), ten Wolde-Frenkel
 clustering (>= 5 neighbours within 1.5 sigma) every 50 steps; a bench step =
-one analysis cycle of 50 steps.  Accelerations stay FP64 in memory (144 B per
-atom-step).
+one analysis cycle of 50 steps.
 
---impl reference times the serial C restatement of the reference (the
-reference is Fortran 77 and no Fortran compiler exists on either machine) on
-the same workload, rank 0 only.
+--impl reference runs the serial C restatement of the reference (the
+reference is Fortran 77 and no Fortran compiler exists on either machine),
+rank 0 only, on one pinned core: for the batched workload each bench step
+is one 100-step window of the 16-replica stratified sample (inputs from the
+oracle's own copy of the start generator: the engine library is never
+loaded), plus an all-core figure under an extra key.
 
 Multi-GPU: independent replicas per rank (seeds offset by rank); the path has
 no data exchange; value = all ranks' atom-steps / max-over-ranks time.
@@ -523,73 +536,153 @@ def dropin_rate(n, rho, temp, seed, steps=300):
     return n * steps / (ms / 1e3)
 
 
-def oracle_rate(n, rho, temp, seed, steps=100, budget_s=4.0):
-    """atom-steps/s of the serial C restatement (all-pairs list, NH,
-    Stillinger every 100 steps) on one replica, one core."""
-    sys.path.insert(0, ORACLE)
-    import orc
-    cfg = nh_config(n, rho, temp)
-    st = make_state(cfg, seed, temp)
-    o = orc.Oracle(cfg, neighbor_mode=0)
-    o.set_state(st, scalars=orc.scalars_init(cfg))
-    o.stopdead(-1)
-    o.neighbor(0)
-    o.zero_acc()
-    o.accatom()
-    s = o.scalars()
-    s.psi = (2.0 * s.ekin - 3.0 * n * CIKB_ * cfg.att) / cfg.Q
-    o.set_scalars(s)
-    o.stoddard(-1)
-    t0 = time.perf_counter()
-    done = 0
-    chunk = 10
-    while done < steps and time.perf_counter() - t0 < budget_s:
-        o.run(done, chunk)
-        done += chunk
-    el = time.perf_counter() - t0
-    o.close()
-    return n * done / el
+# ---------------------------------------------------------------------------
+# The reference's serial algorithm on the host (the oracle: a C restatement of
+# the Fortran, all-pairs neighbour list, Nose-Hoover, Stillinger every 100
+# steps, chk_nucleation), on a fixed sample of the ensemble's replicas.  It
+# builds its inputs with the oracle's own copy of the start generator, so a
+# process that runs only this never loads the engine library.
+# ---------------------------------------------------------------------------
+ORACLE_SAMPLE = 16  # replicas, one per 1/16 quantile of the size distribution
 
 
-CIKB_ = clmd.CIKB
+def oracle_sample_specs(specs, k=ORACLE_SAMPLE):
+    """The replicas at the midpoints of k equal size strata (sorted by N)."""
+    order = sorted(range(len(specs)), key=lambda i: (specs[i][0], i))
+    return [specs[order[int((2 * q + 1) / (2 * k) * (len(order) - 1))]] for q in range(k)]
 
 
-def _oracle_rate_task(task):
-    """One replica's oracle rate (a pool task: spawned processes)."""
-    n, rho, temp, sd, budget = task
-    return n, oracle_rate(n, rho, temp, sd, budget_s=budget)
+class OracleSample:
+    """The sample's replicas on the oracle, advanced window by window
+    (main.f's loop: stoddard + chk_nucleation every 100 steps, then the
+    integrator), each from the start sequence the engine runs at admission
+    (stopdead, neighbor(0), AccAtom, the NH PSI start, stoddard(-1))."""
+
+    def __init__(self, sample):
+        sys.path.insert(0, ORACLE)
+        import orc
+        self.reps = []
+        for n, rho, temp, sd in sample:
+            cfg = nh_config(n, rho, temp)
+            L = cfg.boxx
+            x, y, z, vx, vy, vz = orc.init_random(n, (L, L, L), 0.9, temp, sd)
+            z0 = np.zeros(n)
+            o = orc.Oracle(cfg, neighbor_mode=0)
+            o.set_state(clmd.State(x, y, z, vx, vy, vz, z0, z0, z0),
+                        scalars=orc.scalars_init(cfg))
+            o.stopdead(-1)
+            o.neighbor(0)
+            o.zero_acc()
+            o.accatom()
+            sc = o.scalars()
+            sc.psi = (2.0 * sc.ekin - 3.0 * n * clmd.CIKB * cfg.att) / cfg.Q  # main.f:96-101
+            sc.s = 0.0
+            o.set_scalars(sc)
+            o.stoddard(-1)
+            self.reps.append([o, n, 0, False])  # oracle, N, next step, stopped
+
+    def window(self, steps=100):
+        """One window of every running replica: (seconds, atom-steps)."""
+        done = 0
+        t0 = time.perf_counter()
+        for r in self.reps:
+            o, n, step, stopped = r
+            if stopped:
+                continue
+            st, nxt = o.run(step, steps)
+            if st or nxt < 0 or o.scalars().status:  # nucleated (chk_nucleation) or failed
+                nxt = abs(nxt)
+                r[3] = True
+            done += n * (nxt - step)
+            r[2] = nxt
+        return time.perf_counter() - t0, done
+
+    def atoms(self):
+        return sum(r[1] for r in self.reps)
+
+    def close(self):
+        for r in self.reps:
+            r[0].close()
 
 
-def cpu_ensemble_estimate(specs, budget_s=12.0, cores=1):
-    """The reference algorithm on the batched workload: per-replica rates of
-    the serial oracle on replicas at the size quantiles, interpolated in log N
-    over every replica of the ensemble.  cores > 1: that many processes run
-    replicas at once (the replicas are independent, so a host runs one per
-    core), each rate is measured with all of them busy, and the ensemble's
-    replicas are spread over the cores."""
-    order = sorted(range(len(specs)), key=lambda k: specs[k][0])
-    picks = [order[int(q * (len(order) - 1))] for q in (0.05, 0.35, 0.65, 0.95)]
-    if cores <= 1:
-        rates = [(specs[k][0], oracle_rate(*specs[k], budget_s=budget_s / 4)) for k in picks]
-    else:
-        import multiprocessing as mp
-        tasks = [(*specs[picks[c % len(picks)]], budget_s / 4) for c in range(cores)]
-        with mp.get_context("spawn").Pool(cores) as pool:
-            got = pool.map(_oracle_rate_task, tasks)
-        by_n = {}
-        for n, r in got:
-            by_n.setdefault(n, []).append(r)
-        rates = sorted((n, float(np.mean(v))) for n, v in by_n.items())
-    ln = np.log([r[0] for r in rates])
-    lr = np.log([r[1] for r in rates])
-    t = sum(n / float(np.exp(np.interp(np.log(n), ln, lr))) for n, _, _, _ in specs)
-    value = cores * sum(sp[0] for sp in specs) / t  # per step of every replica
-    desc = ("oracle (serial restatement: all-pairs list, Nose-Hoover, Stillinger every 100 "
-            f"steps) on {cores} core(s): replicas of N = {[r[0] for r in rates]} run for up to "
-            f"100 steps each ({[round(r[1]) for r in rates]} atom-steps/s per core), rates "
-            f"interpolated in log N over all {len(specs)} replicas"
-            + (", spread over the cores" if cores > 1 else ", run one after another"))
-    return value, desc
+def pin_one_core():
+    """Pins this process to one host core (the first it may use)."""
+    try:
+        core = min(os.sched_getaffinity(0))
+        os.sched_setaffinity(0, {core})
+        return core
+    except (AttributeError, OSError):
+        return None
+
+
+def oracle_sample_run(sample, warm, timed, pin=True):
+    """warm + timed windows of the sample on one pinned core: (atom-steps/s
+    over the timed windows, per-window seconds, description)."""
+    core = pin_one_core() if pin else None
+    os_ = OracleSample(sample)
+    for _ in range(warm):
+        os_.window()
+    secs, work = [], 0
+    for _ in range(timed):
+        t, w = os_.window()
+        secs.append(t)
+        work += w
+    os_.close()
+    rate = work / max(sum(secs), 1e-12)
+    desc = (f"oracle (serial C restatement of the reference: all-pairs list, Nose-Hoover, "
+            f"Stillinger + chk_nucleation every 100 steps) on 1 core (cpu {core}), "
+            f"{len(sample)} replicas at the midpoints of 16 size strata of the ensemble "
+            f"(N = {sorted(sp[0] for sp in sample)}, {sum(sp[0] for sp in sample)} atoms), "
+            f"{timed} timed 100-step windows after {warm} untimed")
+    return rate, secs, desc
+
+
+def _oracle_child(sample, warm, timed, q):
+    q.put(oracle_sample_run(sample, warm, timed))
+
+
+def oracle_sample_in_child(sample, warm, timed):
+    """oracle_sample_run in a spawned process (its own pinned core; the
+    caller's threads and GPU context stay as they are)."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    p = ctx.Process(target=_oracle_child, args=(sample, warm, timed, q))
+    p.start()
+    out = q.get()
+    p.join()
+    return out
+
+
+def _oracle_core_worker(sample, core, barrier, q):
+    try:
+        os.sched_setaffinity(0, {core})
+    except (AttributeError, OSError):
+        pass
+    os_ = OracleSample(sample)
+    os_.window()  # untimed
+    barrier.wait()
+    t, w = os_.window()
+    os_.close()
+    q.put((t, w))
+
+
+def oracle_all_cores(sample):
+    """Every host core runs its own copy of the sample for one timed window
+    at the same time (the reference is serial: a host runs independent
+    replicas side by side): whole-host atom-steps / the slowest core's time."""
+    import multiprocessing as mp
+    cores = sorted(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else [0]
+    ctx = mp.get_context("spawn")
+    barrier = ctx.Barrier(len(cores))
+    q = ctx.Queue()
+    ps = [ctx.Process(target=_oracle_core_worker, args=(sample, c, barrier, q)) for c in cores]
+    for p in ps:
+        p.start()
+    got = [q.get() for _ in ps]
+    for p in ps:
+        p.join()
+    return sum(w for _, w in got) / max(t for t, _ in got), len(cores)
 
 
 def batched_reference_arm(args):
@@ -597,25 +690,41 @@ def batched_reference_arm(args):
     if rank != 0:
         return
     specs = ensemble_specs(args.replicas, ENSEMBLE["seed"])
-    budget = min(12.0, max(2.0, 150.0 / max(1, args.warmup + args.steps)))
-    vals, desc = [], ""
-    cores = os.cpu_count() or 1
-    for k in range(args.warmup + args.steps):
-        v, desc = cpu_ensemble_estimate(specs, budget_s=budget, cores=cores)
-        if k >= args.warmup:
-            vals.append(v)
-    value = statistics.mean(vals)
-    total = sum(sp[0] for sp in specs)
+    sample = oracle_sample_specs(specs)
+    all_rate, ncores = (None, None)
+    if not args.no_all_cores:
+        all_rate, ncores = oracle_all_cores(sample)
+    core = pin_one_core()
+    os_ = OracleSample(sample)
+    for _ in range(args.warmup):
+        os_.window()
+    secs, work = [], 0
+    for _ in range(args.steps):
+        t, w = os_.window()
+        secs.append(t)
+        work += w
+    os_.close()
+    value = work / sum(secs)
+    desc = (f"oracle (serial C restatement of the reference: all-pairs list, Nose-Hoover, "
+            f"Stillinger + chk_nucleation every 100 steps) on 1 core (cpu {core}), "
+            f"{len(sample)} replicas at the midpoints of 16 size strata of the ensemble "
+            f"(N = {sorted(sp[0] for sp in sample)}), one bench step = one 100-step window "
+            f"of each")
     line = {
         "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": total * 100 / value * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": batched_config_json(args, total, [0, 0, 0, 0], 1),
-        "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": cores, "kind": "port",
+        "ms_per_step": sum(secs) / len(secs) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": batched_config_json(args, sum(sp[0] for sp in specs), [0, 0, 0, 0], 1),
+        "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": 1, "kind": "port",
                          "sample": desc},
         "e2e": {"value": value, "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "sample_atom_steps_per_step": work / len(secs),
+        "all_cores": ({"value": all_rate, "unit": "atom-steps/s", "cores": ncores,
+                       "how": "one copy of the sample per core at once, one timed window, "
+                              "whole-host atom-steps / slowest core's time"}
+                      if all_rate else None),
     }
     print(json.dumps(line), flush=True)
 
@@ -631,49 +740,97 @@ def batched_config_json(args, total, tuned, ngpu):
             "parallelism": f"replicas x{ngpu}"}
 
 
-def precision_check(specs, nsample=64, windows=20):
-    """The same replicas run twice, mixed and all-FP64 ensembles, for
-    windows x 100 Nose-Hoover steps: the relative drift of each replica's
-    conserved H = ekin + epot + Q PSI^2 / 2 + 3 N kT s (per 1e4 steps; the
-    reference's unshifted cut-off makes H drift in FP64 too) and the
-    cluster-size distribution at the end (sizes of every cluster of every
-    replica, Stillinger 1.5 sigma) compared as a total variation distance."""
+U_RC = 4.0 * (2.5 ** -12 - 2.5 ** -6)  # the LJ pair energy at the cut-off (sigma = eps = 1)
+
+
+def pairs_within(st, box, rc=2.5):
+    """Pairs nearer than rc (minimum image) in a replica's positions."""
+    from scipy.spatial import cKDTree
+    p = np.mod(np.stack([st.x, st.y, st.z], 1), box)
+    p[p >= box] = 0.0
+    return len(cKDTree(p, boxsize=box).query_pairs(rc))
+
+
+def precision_check(specs, nsample=64, windows=100):
+    """Energy drift and cluster sizes of mixed precision against FP64, replica
+    by replica.  The same nsample replicas run three times -- mixed, FP64 and
+    an FP64 twin whose start differs by 1e-13 in one velocity -- for 100 +
+    windows x 100 Nose-Hoover steps.  Per replica the drift of the conserved
+    H = ekin + epot + Q PSI^2/2 + 3 N kT s (main.f:106,142) from step 100 to
+    the end is taken twice: with the reference's epot, whose unshifted
+    cut-off adds U(rc) to H at every pair that crosses rc (so H changes
+    while the vapour condenses even with exact arithmetic), and with the
+    energy the truncated force conserves, H - U(rc) x (pairs within rc).
+    Reported: the mixed - FP64 difference per replica against the twin's
+    (the spread chaos alone gives), and the cluster-size distribution at the
+    end (every cluster of every replica) as a total variation distance."""
     sample = specs[:nsample]
-    out = {}
-    for prec, name in ((clmd.PREC_MIXED, "mixed"), (clmd.PREC_FP64, "fp64")):
+    runs = {}
+    for name, prec, twin in (("mixed", clmd.PREC_MIXED, False), ("fp64", clmd.PREC_FP64, False),
+                             ("fp64_twin", clmd.PREC_FP64, True)):
         e = clmd.Ensemble(clmd.ens_config(sum(n for n, _, _, _ in sample) + 64, len(sample),
                                           precision=prec, integrator=clmd.INT_NOSE,
                                           ftcsi=ENSEMBLE["ftcsi"], threads=256))
-        slots = {}
+        slots = []
         for n, rho, temp, sd in sample:
             box = (n / rho) ** (1.0 / 3.0)
             x, y, z, vx, vy, vz = clmd.init_random(n, (box, box, box), 0.9, temp, sd)
-            slots[e.add(n, box, temp, x, y, z, vx, vy, vz, csover=10**6, budget=0)] = (n, temp)
+            if twin:
+                vx = vx.copy()
+                vx[1] *= 1.0 + 1e-13
+            slots.append(e.add(n, box, temp, x, y, z, vx, vy, vz, csover=10**6, budget=0))
 
         def H(r, n, temp):
             return r.ekin + r.epot + 0.5 * (n * temp * 0.25) * r.psi ** 2 + 3.0 * n * temp * r.s
 
         e.step(1)  # the start sequence and a first window: energies defined
-        h0 = {k: H(r, *slots[k]) for k, r in e.results().items()}
+        res0 = e.results()
+        h0, hs0 = [], []
+        for k, (n, rho, temp, _) in zip(slots, sample):
+            st, _ = e.state(k)
+            h0.append(H(res0[k], n, temp))
+            hs0.append(h0[-1] - U_RC * pairs_within(st, (n / rho) ** (1.0 / 3.0)))
         e.step(windows)
         res = e.results()
-        drift = [abs(H(res[k], *slots[k]) - h0[k]) / abs(h0[k]) * 1e4 / (windows * 100)
-                 for k in slots]
-        sizes = []
-        for k in slots:
-            _, cl = e.state(k)
-            sizes.extend(np.bincount(cl)[1:][np.bincount(cl)[1:] > 0].tolist())
-        out[name] = (float(np.median(drift)), np.bincount(sizes))
+        d, ds, sizes = [], [], []
+        for j, (k, (n, rho, temp, _)) in enumerate(zip(slots, sample)):
+            st, cl = e.state(k)
+            h = H(res[k], n, temp)
+            hs = h - U_RC * pairs_within(st, (n / rho) ** (1.0 / 3.0))
+            d.append((h - h0[j]) / abs(h0[j]))
+            ds.append((hs - hs0[j]) / abs(hs0[j]))
+            c = np.bincount(cl)[1:]
+            sizes.extend(c[c > 0].tolist())
+            assert res[k].status == 0, (name, k, res[k].status)
+        runs[name] = (np.array(d), np.array(ds), np.bincount(sizes))
         e.close()
-    a, b = out["mixed"][1], out["fp64"][1]
-    m = max(len(a), len(b))
-    pa = np.pad(a, (0, m - len(a))).astype(float)
-    pb = np.pad(b, (0, m - len(b))).astype(float)
+    dm, dsm, hm = runs["mixed"]
+    df, dsf, hf = runs["fp64"]
+    dt, dst, _ = runs["fp64_twin"]
+    gap, chaos = np.abs(dm - df), np.abs(dt - df)
+    m = max(len(hm), len(hf))
+    pa = np.pad(hm, (0, m - len(hm))).astype(float)
+    pb = np.pad(hf, (0, m - len(hf))).astype(float)
     tv = 0.5 * np.abs(pa / pa.sum() - pb / pb.sum()).sum()
-    return {"replicas": nsample, "steps": windows * 100,
-            "energy_drift_per_1e4_steps_median": {"mixed": out["mixed"][0],
-                                                   "fp64": out["fp64"][0]},
-            "cluster_size_distribution_tv_distance": float(tv)}
+    steps = windows * 100
+    return {
+        "replicas": nsample, "steps": steps, "from_step": 100,
+        "relative_drift_of_H": {
+            "mixed_median": float(np.median(np.abs(dm))),
+            "fp64_median": float(np.median(np.abs(df))),
+            "mixed_minus_fp64_median": float(np.median(gap)),
+            "mixed_minus_fp64_max": float(gap.max()),
+            "fp64_twin_minus_fp64_median": float(np.median(chaos)),
+            "fp64_twin_minus_fp64_max": float(chaos.max()),
+            "replicas_within_3x_twin_spread_plus_1e-6": int((gap <= 3 * chaos + 1e-6).sum())},
+        "relative_drift_of_shifted_H": {
+            "mixed_median": float(np.median(np.abs(dsm))),
+            "mixed_max": float(np.abs(dsm).max()),
+            "fp64_median": float(np.median(np.abs(dsf))),
+            "fp64_max": float(np.abs(dsf).max()),
+            "fp64_twin_max": float(np.abs(dst).max()),
+            "replicas_mixed_within_1e-4": int((np.abs(dsm) <= 1e-4).sum())},
+        "cluster_size_distribution_tv_distance": float(tv)}
 
 
 def mixed_force_error(e, slots, specs_by_slot, nsample=3):
@@ -784,8 +941,16 @@ def batched_arm(args):
     d2h = 6 * 8 * total + 16 * len(slots)
 
     line = None
+    extra = {}
     if rank == 0:
         ferr_n, ferr_a = mixed_force_error(e, slots, slots)
+    e.close()
+    rk.barrier()
+    # ---- the same replicas as an all-FP64 ensemble (same kernels, FP64
+    # pair terms and sums): how much of the gain is batching, how much
+    # mixed precision
+    fp64_value, fp64_tuned = fp64_ensemble_rate(specs, args)
+    if rank == 0:
         pcheck = precision_check(specs)
         order = sorted(slots, key=lambda k: slots[k][0])
         picks = [order[int(q * (len(order) - 1))] for q in np.linspace(0, 1, args.dropin_sample)]
@@ -795,11 +960,16 @@ def batched_arm(args):
         t_drop = sum(slots[k][0] * 100 / float(np.exp(np.interp(np.log(slots[k][0]), ln, lr)))
                      for k in slots)
         dropin_value = sum(slots[k][0] * 100 for k in slots) / t_drop
+        extra = dict(pcheck=pcheck, rates=rates, dropin_value=dropin_value)
+    # ---- served leg: a bounded Poisson window on this GPU
+    served = None if args.no_served else served_leg(args, rk)
+    if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            v, desc = cpu_ensemble_estimate(specs)
+            v, secs, desc = oracle_sample_in_child(oracle_sample_specs(specs), 1, 3)
             cpu = {"value": v, "unit": "atom-steps/s", "cores": 1, "kind": "port",
-                   "sample": desc}
+                   "sample": desc, "seconds_per_window": secs}
+        dropin_value = extra["dropin_value"]
         line = {
             "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": el_max / args.steps * 1e3,
@@ -818,16 +988,48 @@ def batched_arm(args):
                          "peak_kind": peak_kind},
             "cpu_baseline": cpu,
             "clocks": clk,
+            "fp64_ensemble_same_ensemble": fp64_value,
+            "fp64_ensemble_threads_per_size_class": [clmd.shape_name(t) for t in fp64_tuned],
+            "speedup_vs_fp64_ensemble": value / fp64_value,
             "fp64_dropin_same_ensemble": dropin_value,
             "speedup_vs_fp64_dropin": value / dropin_value,
-            "dropin_sample_rates": [[n, r] for n, r in rates],
+            "dropin_sample_rates": [[n, r] for n, r in extra["rates"]],
             "force_rel_err_vs_fp64": {"normwise": ferr_n, "worst_atom": ferr_a},
-            "mixed_vs_fp64_sample": pcheck,
+            "mixed_vs_fp64_sample": extra["pcheck"],
             "nucleated": sum(1 for r in res.values() if r.done == 1),
+            "served": served,
         }
         print(json.dumps(line), flush=True)
-    e.close()
     rk.close()
+
+
+def fp64_ensemble_rate(specs, args, windows=3):
+    """atom-steps/s of the all-FP64 ensemble on the same replicas (whole
+    windows, after the start window and the tuner)."""
+    import torch
+    total = sum(sp[0] for sp in specs)
+    e = clmd.Ensemble(clmd.ens_config(total + 1024, len(specs), precision=clmd.PREC_FP64,
+                                      integrator=clmd.INT_NOSE, ftcsi=ENSEMBLE["ftcsi"],
+                                      threads=args.threads))
+    for n, rho, temp, sd in specs:
+        box = (n / rho) ** (1.0 / 3.0)
+        x, y, z, vx, vy, vz = clmd.init_random(n, (box, box, box), 0.9, temp, sd)
+        e.add(n, box, temp, x, y, z, vx, vy, vz, csover=ENSEMBLE["csover"], clwait=0,
+              budget=ENSEMBLE["budget"])
+    e.step(1)
+    tuned = e.autotune() if args.threads == 0 else [args.threads] * 4
+    e.step(1)
+    r0 = {k: v.step for k, v in e.results().items()}
+    torch.cuda.synchronize()
+    t = time.perf_counter()  # timed like the mixed value: whole windows, host clock
+    for _ in range(windows):
+        e.step(1)
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t
+    res = e.results()
+    work = sum(e.natom[k] * (res[k].step - r0[k]) for k in res)
+    e.close()
+    return work / el, tuned
 
 
 # served solves: Poisson arrivals, continuous batching (clmd_serve)
@@ -870,20 +1072,19 @@ def served_config_json(args, nreq, pool, ngpu):
             "parallelism": f"independent traces x{ngpu}"}
 
 
-def served_arm(args):
+def run_served(args, rk, arrival_s, serve_s, max_slots):
+    """One served trace on this rank's GPU: the atom pool from free HBM, a
+    short untimed trace first (block shapes, code paths), then the Poisson
+    trace.  Returns (results, stats, clocks, launches, pool atoms, requests)."""
     import torch
-
-    rk = Ranks(timeout_s=600)
-    rank, world, dev = rk.rank, rk.world, rk.device
-    clmd.set_device(dev)
+    dev = rk.device
     free, _ = torch.cuda.mem_get_info(dev)
     pool = int(min(args.pool_fraction * free / POOL_BYTES_PER_ATOM, 2**31 - 1))
-    reqs = served_trace(args.arrival_seconds, SERVED["seed"] + 1000 * rank)
-    e = clmd.Ensemble(clmd.ens_config(pool, 16384, precision=clmd.PREC_MIXED,
+    reqs = served_trace(arrival_s, SERVED["seed"] + 1000 * rk.rank)
+    e = clmd.Ensemble(clmd.ens_config(pool, max_slots, precision=clmd.PREC_MIXED,
                                       integrator=clmd.INT_NOSE, ftcsi=SERVED["ftcsi"],
                                       threads=args.threads or 0))
-    # block sizes per size class from a short tuning trace (not timed)
-    warm = served_trace(0.25, SERVED["seed"] + 999 + 1000 * rank)
+    warm = served_trace(0.25, SERVED["seed"] + 999 + 1000 * rk.rank)
     for r in warm:
         r.arrival = 0.0
         r.budget = 400
@@ -892,58 +1093,98 @@ def served_arm(args):
     clocks = Clocks(dev)
     l0 = e.launches()
     clocks.start()
-    out, st = e.serve(reqs, args.serve_seconds)
+    out, st = e.serve(reqs, serve_s)
     clk = clocks.stop()
     launches = e.launches() - l0
+    e.close()
+    return out, st, clk, launches, pool, reqs
 
+
+def served_summary(out, st, nreq, serve_s):
+    """Latency percentiles of a served trace.  A request still running when
+    the loop stops is censored: its latency is at least (stop - arrival), so
+    a percentile that reaches into the censored ones is a lower bound."""
+    lat = np.array([o.finished - o.arrival for o in out if o.done in (1, 2)])
+    nuc = np.array([o.finished - o.arrival for o in out if o.done == 1])
+    nuc_steps = np.array([o.clbrkt for o in out if o.done == 1])
+    wait = np.array([o.admitted - o.arrival for o in out if o.admitted >= 0])
+    unfinished = [o for o in out if o.done == 0]
+    # every request, the censored ones at their lower bound
+    lat_all = np.array([o.finished - o.arrival if o.done in (1, 2) else st.wall - o.arrival
+                        for o in out])
+
+    def pct(a, q):
+        return float(np.percentile(a, q)) if len(a) else None
+    cens = len(unfinished) / max(1, len(out))
+    return {
+        "latency_s": {"p50": pct(lat_all, 50), "p99": pct(lat_all, 99),
+                      "p50_is_lower_bound": cens > 0.5, "p99_is_lower_bound": cens > 0.01,
+                      "completed_p50": pct(lat, 50), "completed_p99": pct(lat, 99),
+                      "time_to_nucleation_p50": pct(nuc, 50),
+                      "time_to_nucleation_p99": pct(nuc, 99),
+                      "nucleation_step_p50": pct(nuc_steps, 50),
+                      "nucleation_step_p99": pct(nuc_steps, 99),
+                      "admission_wait_p50": pct(wait, 50), "admission_wait_p99": pct(wait, 99)},
+        "requests": {"arrived": nreq, "admitted": st.admitted, "completed": st.completed,
+                     "nucleated": int(len(nuc)), "censored": len(unfinished),
+                     "peak_resident": st.peak_resident, "peak_atoms": int(st.peak_atoms)},
+        "wall_s": st.wall, "serve_cap_s": serve_s,
+    }
+
+
+def served_leg(args, rk):
+    """configs[4] inside the default bench: a bounded Poisson window at 200
+    requests/s (N log-uniform in [100, 50000], rho* and T* uniform, budgets
+    log-uniform in [1e4, 1e6], threshold largest cluster > 100), served with
+    continuous batching on this GPU until every request finished or the cap
+    passed.  Aggregate atom-steps/s and the latency percentiles."""
+    out, st, clk, launches, pool, reqs = run_served(args, rk, args.served_arrival,
+                                                    args.served_cap, args.served_slots)
+    units = rk.sum(st.atom_steps)
+    wall = rk.max(st.wall)
+    d = {"workload": f"served-poisson-{SERVED['rate']:.0f}req/s-for-{args.served_arrival}s"
+                     "(N=100..50000 log-uniform, rho*=0.01..0.05, T*=0.65..0.85, budget "
+                     "1e4..1e6 log-uniform, stop at largest cluster > 100)-NoseHoover-mixed",
+         "value": units / wall, "unit": "atom-steps/s", "gpu_launches": int(launches),
+         "pool_atoms": pool, "max_resident_replicas": args.served_slots, "clocks": clk}
+    d.update(served_summary(out, st, len(reqs), args.served_cap))
+    return d
+
+
+def served_arm(args):
+    rk = Ranks(timeout_s=600)
+    clmd.set_device(rk.device)
+    out, st, clk, launches, pool, reqs = run_served(args, rk, args.arrival_seconds,
+                                                    args.serve_seconds, args.served_slots)
     wall = rk.max(st.wall)
     units = rk.sum(st.atom_steps)
     value = units / wall
-    if rank == 0:
-        lat = np.array([o.finished - o.arrival for o in out if o.done in (1, 2)])
-        nuc = np.array([o.finished - o.arrival for o in out if o.done == 1])
-        wait = np.array([o.admitted - o.arrival for o in out if o.admitted >= 0])
-        unfinished = sum(1 for o in out if o.done == 0)
-
-        def pct(a, q):
-            return float(np.percentile(a, q)) if len(a) else None
-        # a percentile over all requests is a lower bound while requests past
-        # it are still running when the window closes
-        censored_p99 = unfinished > 0.01 * len(out)
+    if rk.rank == 0:
         admitted_atoms = sum(o.natom for o in out if o.admitted >= 0)
         cpu = None
-        if world == 1 and not args.no_cpu_baseline:
+        if rk.world == 1 and not args.no_cpu_baseline:
             specs = [(r.natom, r.rho, r.temp, r.seed) for r in reqs]
-            v, desc = cpu_ensemble_estimate(specs)
+            v, secs, desc = oracle_sample_in_child(oracle_sample_specs(specs), 1, 2)
             cpu = {"value": v, "unit": "atom-steps/s", "cores": 1, "kind": "port",
-                   "sample": desc}
+                   "sample": desc, "seconds_per_window": secs}
         line = {
             "metric": "atom-steps/s (served)", "value": value, "unit": "atom-steps/s",
-            "n_gpus": world, "steps": st.windows, "warmup": 1,
+            "n_gpus": rk.world, "steps": st.windows, "warmup": 1,
             "ms_per_step": wall / max(1, st.windows) * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic (seeded Poisson trace)",
-            "config": served_config_json(args, len(reqs), pool, world),
+            "config": served_config_json(args, len(reqs), pool, rk.world),
             "e2e": {"value": value, "unit": "atom-steps/s",
                     "h2d_bytes_per_step": 48 * admitted_atoms / max(1, st.windows),
                     "d2h_bytes_per_step": 16 * st.peak_resident,
                     "note": "the served loop is end to end: host start states in, "
                             "per-window status out, wall clock"},
-            "latency_s": {"p50": pct(lat, 50), "p99": pct(lat, 99),
-                          "p99_is_lower_bound": censored_p99,
-                          "time_to_nucleation_p50": pct(nuc, 50),
-                          "time_to_nucleation_p99": pct(nuc, 99),
-                          "admission_wait_p50": pct(wait, 50), "admission_wait_p99": pct(wait, 99)},
-            "requests": {"arrived": len(reqs), "admitted": st.admitted,
-                         "completed": st.completed, "nucleated": int(len(nuc)),
-                         "unfinished": unfinished, "peak_resident": st.peak_resident,
-                         "peak_atoms": int(st.peak_atoms)},
             "gpu_launches": int(launches),
             "cpu_baseline": cpu,
             "clocks": clk,
         }
+        line.update(served_summary(out, st, len(reqs), args.serve_seconds))
         print(json.dumps(line), flush=True)
-    e.close()
     rk.close()
 
 
@@ -953,22 +1194,17 @@ def served_reference_arm(args):
         return
     reqs = served_trace(args.arrival_seconds, SERVED["seed"])
     specs = [(r.natom, r.rho, r.temp, r.seed) for r in reqs]
-    vals, desc = [], ""
-    cores = os.cpu_count() or 1
-    for k in range(max(1, args.warmup // 3) + 1):
-        v, desc = cpu_ensemble_estimate(specs, cores=cores)
-        if k > 0:
-            vals.append(v)
-    value = statistics.mean(vals)
+    v, secs, desc = oracle_sample_run(oracle_sample_specs(specs), args.warmup, args.steps)
     line = {
-        "metric": "atom-steps/s (served)", "value": value, "unit": "atom-steps/s",
-        "impl": "reference", "n_gpus": args.gpus, "steps": len(vals), "warmup": 1,
-        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic (seeded Poisson trace)",
+        "metric": "atom-steps/s (served)", "value": v, "unit": "atom-steps/s",
+        "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": sum(secs) / len(secs) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Poisson trace)",
         "config": served_config_json(args, len(reqs), 0, 1),
-        "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": cores, "kind": "port",
+        "cpu_baseline": {"value": v, "unit": "atom-steps/s", "cores": 1, "kind": "port",
                          "sample": desc},
-        "e2e": {"value": value, "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
+        "e2e": {"value": v, "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -982,6 +1218,8 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--natom", type=int, default=0, help="dropin/nvt: atoms (0 = the workload's)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-all-cores", action="store_true",
+                    help="reference arm: skip the all-core figure")
     ap.add_argument("--workload", default="batched",
                     choices=["batched", "dropin", "nvt", "served"])
     ap.add_argument("--arrival-seconds", type=float, default=1.0,
@@ -993,6 +1231,14 @@ def main():
     ap.add_argument("--replicas", type=int, default=4096)
     ap.add_argument("--threads", type=int, default=0, help="0 = autotune")
     ap.add_argument("--dropin-sample", type=int, default=8)
+    ap.add_argument("--no-served", action="store_true",
+                    help="batched: leave out the served leg")
+    ap.add_argument("--served-arrival", type=float, default=10.0,
+                    help="batched: Poisson arrival window of the served leg (s)")
+    ap.add_argument("--served-cap", type=float, default=30.0,
+                    help="batched: wall-clock cap of the served leg (s)")
+    ap.add_argument("--served-slots", type=int, default=16384,
+                    help="served: resident replicas at most (the ensemble's slots)")
     args = ap.parse_args()
     if args.workload == "nvt":
         w = dict(NVT, natom=args.natom or NVT["natom"])

@@ -583,12 +583,21 @@ class System:
 
 
 ENS_LEAN = 0x10000  # CLMD_ENS_LEAN: the 64-register variant of a 128/256/512-thread CTA
+ENS_LANES_SHIFT = 20  # CLMD_ENS_LANES_SHIFT: 1 << field lanes per atom (mixed forces)
+
+
+def ens_lanes(n):
+    """The block-shape bits for n (1, 2 or 4) lanes per atom in the mixed
+    force pass."""
+    return {1: 0, 2: 1, 4: 2}[n] << ENS_LANES_SHIFT
 
 
 def shape_name(shape):
-    """A block shape as text: '256' or '256 lean (64 regs)'."""
+    """A block shape as text: '256', '256 lean (64 regs)', '1024, 2 lanes/atom'."""
     t = shape & 0xFFFF
-    return f"{t} lean (64 regs)" if shape & ENS_LEAN else str(t)
+    out = f"{t} lean (64 regs)" if shape & ENS_LEAN else str(t)
+    lanes = 1 << ((shape >> ENS_LANES_SHIFT) & 3)
+    return out + (f", {lanes} lanes/atom" if lanes > 1 else "")
 
 
 def ens_config(max_atoms, max_replicas, *, precision=PREC_MIXED, integrator=INT_NOSE, ftcsi=100,

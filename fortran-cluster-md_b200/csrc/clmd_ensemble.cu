@@ -20,6 +20,7 @@
 // fixed order (rows ordered by the cell sweep over index-sorted cells), so a
 // replica's result does not depend on which other replicas share the launch.
 // Positions, velocities, PSI, energies and the virial stay FP64.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdio.h>
@@ -35,6 +36,8 @@
 #include "clmd_mixed.cuh"
 
 namespace clmd_ens {
+
+namespace cg = cooperative_groups;
 
 constexpr int kFptCap = 128;  // first-passage sizes tracked per replica
 constexpr int kNcMax = 28;    // cells per dimension at most (cells never narrower than the list radius)
@@ -70,9 +73,14 @@ struct Args {
   int* ctr;
   double rc, atskin, dt;
   int nbtim, ftcsi, lstride, integrator, nwin;
+  int lg;  // mixed force pass: 1 << lg lanes per atom (0: one thread per atom)
   int ncmax;  // cells per dimension this launch's shared memory holds
   int4* summary;  // per slot: done, status, step, maxcs
   float* wtime;   // per slot: device ms per MD step in its last launch (one CTA)
+  // replicas run by a thread-block cluster: each cluster's cell counts and
+  // scatter cursors (kNcMax^3 + 2 ints per cluster, indexed by cluster)
+  int* cscr;
+  long long cscr_stride;
 };
 
 __device__ __forceinline__ double wsum(double v) {
@@ -225,6 +233,8 @@ __device__ __forceinline__ double mi_bf(double d, double L, double iL, double bf
 }
 
 struct Cta {
+  double xred[3 * 16];  // cluster reductions: the CTAs' partials (rank 0's copy is read)
+  double xloc[4];       // cluster reductions: the totals, for this CTA's threads
   double* sx;  // positions in shared memory (nullptr: global)
   double* sy;
   double* sz;
@@ -236,6 +246,139 @@ struct Cta {
   int rep;  // slot of the replica being run
   int nsteps;  // MD steps this replica runs in this launch
 };
+
+// ---------------------------------------------------------------------------
+// A replica runs on one CTA (CS = 1) or on a thread-block cluster of CS CTAs
+// (replicas whose positions do not fit in one SM's shared memory).  Every
+// per-atom loop starts at gtid<NT, CS>() with stride NT * CS; gsync<CS>() is
+// the barrier over the replica's threads (__syncthreads, or the cluster
+// barrier whose release/acquire orders global and shared memory across the
+// cluster); the grp_* reductions add a second level for CS > 1: each CTA's
+// total goes to rank 0's shared memory (distributed shared memory), every
+// CTA sums the CS partials in one fixed tree, so all CTAs hold bit-identical
+// totals and keep identical copies of the replica record.  With CS = 1 the
+// code is exactly the single-CTA code.
+template <int CS>
+__device__ __forceinline__ unsigned grank() {
+  if constexpr (CS == 1)
+    return 0u;
+  else
+    return cg::this_cluster().block_rank();
+}
+template <int NT, int CS>
+__device__ __forceinline__ int gtid() {
+  return (int)grank<CS>() * NT + (int)threadIdx.x;
+}
+template <int CS>
+__device__ __forceinline__ void gsync() {
+  if constexpr (CS == 1)
+    __syncthreads();
+  else
+    cg::this_cluster().sync();
+}
+
+// the cluster level of a reduction of nv values (v[k]: this CTA's totals,
+// the same in every thread): returns the cluster totals in v.  op 0 sums,
+// op 1 takes maxima.  Two cluster barriers: the partials are published, then
+// read by every CTA before any CTA may write the next reduction's.
+template <int CS>
+__device__ __forceinline__ void cl_reduce(double* v, int nv, const int* op, Cta& C) {
+  auto cl = cg::this_cluster();
+  const unsigned r = cl.block_rank();
+  double* b0 = cl.map_shared_rank(C.xred, 0);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < nv; k++) b0[k * 16 + r] = v[k];
+  cl.sync();
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    for (int k = 0; k < nv; k++) {
+      double t = lane < CS ? b0[k * 16 + lane] : (op[k] ? -1.0e300 : 0.0);
+      t = op[k] ? wmax(t) : wsum(t);
+      if (lane == 0) C.xloc[k] = t;
+    }
+  }
+  cl.sync();
+  for (int k = 0; k < nv; k++) v[k] = C.xloc[k];
+}
+
+template <int NT, int CS>
+__device__ __forceinline__ double grp_sum(double v, Cta& C) {
+  double t = cta_sum<NT>(v, C.red);
+  if constexpr (CS > 1) {
+    const int op[1] = {0};
+    cl_reduce<CS>(&t, 1, op, C);
+  }
+  return t;
+}
+template <int NT, int CS>
+__device__ __forceinline__ double grp_max(double v, Cta& C) {
+  double t = cta_max<NT>(v, C.red);
+  if constexpr (CS > 1) {
+    const int op[1] = {1};
+    cl_reduce<CS>(&t, 1, op, C);
+  }
+  return t;
+}
+template <int NT, int CS>
+__device__ __forceinline__ void grp_maxsum(double& a, double& b, Cta& C) {
+  cta_maxsum<NT>(a, b, C.red);
+  if constexpr (CS > 1) {
+    double v[2] = {a, b};
+    const int op[2] = {1, 0};
+    cl_reduce<CS>(v, 2, op, C);
+    a = v[0];
+    b = v[1];
+  }
+}
+template <int NT, int CS>
+__device__ __forceinline__ void grp_sum2(double& a, double& b, int& f, Cta& C) {
+  cta_sum2<NT>(a, b, f, C.red);
+  if constexpr (CS > 1) {
+    double v[3] = {a, b, f ? 1.0 : 0.0};
+    const int op[3] = {0, 0, 1};
+    cl_reduce<CS>(v, 3, op, C);
+    a = v[0];
+    b = v[1];
+    f = v[2] != 0.0;
+  }
+}
+template <int NT, int CS>
+__device__ __forceinline__ int grp_or(int f, Cta& C) {
+  if constexpr (CS == 1) {
+    return __syncthreads_or(f);
+  } else {
+    double v[1] = {(double)__syncthreads_or(f)};
+    const int op[1] = {1};
+    cl_reduce<CS>(v, 1, op, C);
+    return v[0] != 0.0;
+  }
+}
+// the closed-form Nose-Hoover root of the group total of S (cta_nh_root for
+// one CTA; for a cluster the total first, then warp 0 of every CTA takes the
+// same root from the same total)
+template <int NT, int CS>
+__device__ __forceinline__ bool grp_nh_root(double S, double psi1, double nkt3, double dth,
+                                            double Q, Cta& C, double& Stot, double& p) {
+  if constexpr (CS == 1) {
+    return cta_nh_root<NT>(S, psi1, nkt3, dth, Q, C.red, Stot, p);
+  } else {
+    double t = grp_sum<NT, CS>(S, C);
+    if (threadIdx.x < 32) {
+      double pr;
+      const bool ok = clmd_nh_root(t, psi1, nkt3, dth, Q, pr);
+      if (threadIdx.x == 0) {
+        C.red[33] = pr;
+        C.red[34] = ok ? 1.0 : 0.0;
+      }
+    }
+    __syncthreads();
+    Stot = t;
+    p = C.red[33];
+    const bool ok = C.red[34] != 0.0;
+    __syncthreads();
+    return ok;
+  }
+}
 
 template <bool SM>
 struct Pos {
@@ -349,77 +492,92 @@ __device__ void length_order(const Rep& R, Cta& C, const Args& A) {
   }
 }
 
+// exclusive scan in place of cnt[0..n) by one CTA (thread 0 walks the warp
+// sums): cnt[c] becomes the sum of the counts before c
+template <int NT>
+__device__ void cta_scan(int* cnt, int n) {
+  __shared__ int wsums[NT / 32 + 1];
+  const int tid = threadIdx.x;
+  const int per = (n + NT - 1) / NT;
+  int b0 = tid * per, s = 0;
+  for (int k = 0; k < per; k++)
+    if (b0 + k < n) s += cnt[b0 + k];
+  int lane = tid & 31, w = tid >> 5, incl = s;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) wsums[w] = incl;
+  __syncthreads();
+  if (tid == 0) {
+    int acc = 0;
+    for (int k = 0; k < NT / 32; k++) {
+      int t = wsums[k];
+      wsums[k] = acc;
+      acc += t;
+    }
+  }
+  __syncthreads();
+  int ex = wsums[w] + incl - s;
+  for (int k = 0; k < per; k++)
+    if (b0 + k < n) {
+      int v = cnt[b0 + k];
+      cnt[b0 + k] = ex;
+      ex += v;
+    }
+  __syncthreads();
+}
+
 // cell list + rows (ELL, transposed per replica: entry k of atom i at
 // list[off*stride + k*N + i]); cells are index-sorted so row order is fixed
-template <int NT, bool SM>
+template <int NT, bool SM, int CS>
 __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
   const int N = R.natom, off = R.off, tid = threadIdx.x;
+  const int gt = gtid<NT, CS>();
+  constexpr int GT = NT * CS;
   const double L = R.box;
-  // one shared array does the counting sort: counts at cstart[c + 1], an
-  // in-place exclusive scan turns them into starts, and the scatter's
-  // atomics advance each to its cell's end = the next cell's start
-  for (int c = tid; c <= C.ncell; c += NT) C.cstart[c] = 0;
-  __syncthreads();
-  for (int i = tid; i < N; i += NT) {
+  // one array does the counting sort: counts at cnt[c + 1], an in-place
+  // exclusive scan turns them into starts, and the scatter's atomics advance
+  // each to its cell's end = the next cell's start.  One CTA keeps it in
+  // shared memory; a cluster keeps it in global memory (its scratch) and
+  // then copies the result into every CTA's shared memory for the search.
+  int* cnt = C.cstart;
+  if constexpr (CS > 1) cnt = A.cscr + (long long)(blockIdx.x / CS) * A.cscr_stride;
+  for (int c = gt; c <= C.ncell; c += GT) cnt[c] = 0;
+  gsync<CS>();
+  for (int i = gt; i < N; i += GT) {
     const double x = wrap_box(P.x(i), L), y = wrap_box(P.y(i), L), z = wrap_box(P.z(i), L);
     P.set(i, x, y, z);
     int cx = min((int)(x * C.cf), C.ncx - 1), cy = min((int)(y * C.cf), C.ncx - 1),
         cz = min((int)(z * C.cf), C.ncx - 1);
     int c = (cz * C.ncx + cy) * C.ncx + cx;
     A.cellid[off + i] = c;
-    atomicAdd(&C.cstart[c + 1], 1);
+    atomicAdd(&cnt[c + 1], 1);
   }
-  __syncthreads();
-  // exclusive scan of the counts (thread 0 walks warp sums)
-  {
-    __shared__ int wsums[NT / 32 + 1];
-    int* cnt = C.cstart + 1;
-    const int per = (C.ncell + NT - 1) / NT;
-    int b0 = tid * per, s = 0;
-    for (int k = 0; k < per; k++)
-      if (b0 + k < C.ncell) s += cnt[b0 + k];
-    int lane = tid & 31, w = tid >> 5, incl = s;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      int t = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += t;
-    }
-    if (lane == 31) wsums[w] = incl;
-    __syncthreads();
-    if (tid == 0) {
-      int acc = 0;
-      for (int k = 0; k < NT / 32; k++) {
-        int t = wsums[k];
-        wsums[k] = acc;
-        acc += t;
-      }
-    }
-    __syncthreads();
-    int ex = wsums[w] + incl - s;
-    for (int k = 0; k < per; k++)
-      if (b0 + k < C.ncell) {
-        int v = cnt[b0 + k];
-        cnt[b0 + k] = ex;
-        ex += v;
-      }
-    __syncthreads();
-  }
+  gsync<CS>();
+  if (grank<CS>() == 0) cta_scan<NT>(cnt + 1, C.ncell);
+  gsync<CS>();
   // scatter in arrival order (parent[] is free outside the analysis), then
   // each atom takes the place of its rank by index inside its cell: the
   // cell order is fixed whatever the order of the atomics
   int* tmp = A.parent + off;
-  for (int i = tid; i < N; i += NT) {
-    int slot = atomicAdd(&C.cstart[A.cellid[off + i] + 1], 1);
+  for (int i = gt; i < N; i += GT) {
+    int slot = atomicAdd(&cnt[A.cellid[off + i] + 1], 1);
     tmp[slot] = i;
   }
-  __syncthreads();
-  for (int i = tid; i < N; i += NT) {
+  gsync<CS>();
+  if constexpr (CS > 1) {
+    for (int c = tid; c <= C.ncell; c += NT) C.cstart[c] = __ldcg(cnt + c);
+    __syncthreads();
+  }
+  for (int i = gt; i < N; i += GT) {
     const int c = A.cellid[off + i], c0 = C.cstart[c], c1 = C.cstart[c + 1];
     int r = 0;
     for (int q = c0; q < c1; q++) r += tmp[q] < i;
     A.sorted[off + c0 + r] = i;
   }
-  __syncthreads();
+  gsync<CS>();
   if ((!SM && R.reorder == 1) || R.reorder == 2) {
     // reorder 1 (positions in global memory): the atoms move into cell
     // order, so that a warp's neighbour gathers fall within a few cells'
@@ -430,33 +588,35 @@ __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
     // rewrite them), so they hold the gathered copies.  Accelerations are
     // dead too: the force pass after a rebuild writes them before any read.
     const int* srt = A.sorted + off;
-    if (R.reorder == 2) {
-      length_order<NT>(R, C, A);
-      srt = A.cs + off;
+    if constexpr (CS == 1) {
+      if (R.reorder == 2) {
+        length_order<NT>(R, C, A);
+        srt = A.cs + off;
+      }
     }
     double *gx = A.vxn + off, *gy = A.vyn + off, *gz = A.vzn + off;
     int* go = A.parent + off;
-    for (int p = tid; p < N; p += NT) {
+    for (int p = gt; p < N; p += GT) {
       const int q = srt[p];
       gx[p] = P.x(q);
       gy[p] = P.y(q);
       gz[p] = P.z(q);
       go[p] = A.orig[off + q];
     }
-    __syncthreads();
-    for (int p = tid; p < N; p += NT) {
+    gsync<CS>();
+    for (int p = gt; p < N; p += GT) {
       P.set(p, gx[p], gy[p], gz[p]);
       A.orig[off + p] = go[p];
     }
-    __syncthreads();
-    for (int p = tid; p < N; p += NT) {
+    gsync<CS>();
+    for (int p = gt; p < N; p += GT) {
       const int q = srt[p];
       gx[p] = A.vx[off + q];
       gy[p] = A.vy[off + q];
       gz[p] = A.vz[off + q];
     }
-    __syncthreads();
-    for (int p = tid; p < N; p += NT) {
+    gsync<CS>();
+    for (int p = gt; p < N; p += GT) {
       A.vx[off + p] = gx[p];
       A.vy[off + p] = gy[p];
       A.vz[off + p] = gz[p];
@@ -465,12 +625,12 @@ __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
       else
         A.sorted[off + p] = p;  // the cells now hold consecutive slots
     }
-    __syncthreads();
+    gsync<CS>();
   }
   const double hL = 0.5 * L, rs2 = C.rs2;
   const long long lbase = (long long)off * A.lstride;
   int over = 0;
-  for (int i = tid; i < N; i += NT) {
+  for (int i = gt; i < N; i += GT) {
     const double xi = P.x(i), yi = P.y(i), zi = P.z(i);
     int cx = min((int)(xi * C.cf), C.ncx - 1), cy = min((int)(yi * C.cf), C.ncx - 1),
         cz = min((int)(zi * C.cf), C.ncx - 1);
@@ -534,10 +694,10 @@ __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
     }
     A.rlen[off + i] = n;
   }
-  over = __syncthreads_or(over);
+  over = grp_or<NT, CS>(over, C);
   if (over) {
     if (tid == 0 && R.status == 0) R.status = CLMD_ERR_LIST_OVERFLOW;
-    __syncthreads();
+    gsync<CS>();
     return false;
   }
   return true;
@@ -558,15 +718,89 @@ __device__ int skin(Rep& R, const Args& A, double dmmr) {
 // velocity-Verlet second half kick; FP64 energy/virial sums when asked
 // NHF: also the Nose-Hoover solve's first pass on the fresh accelerations
 // (vo = v: vxn = v, s0 += v.v, dp += b vo dt/Q with b = -dth (a - psi1 vo))
-template <int NT, bool SM, bool MIXED, bool NHF = false>
+template <int NT, bool SM, bool MIXED, int CS, bool NHF = false>
 __device__ void forces(Rep& R, Cta& C, const Args& A, const Pos<SM>& P, bool kick,
                        bool energies, double psi1 = 0.0, double dtQ = 0.0, double* s0 = nullptr,
                        double* dp = nullptr) {
   const int N = R.natom, off = R.off, tid = threadIdx.x;
+  const int gt = gtid<NT, CS>();
+  constexpr int GT = NT * CS;
   const double L = R.box, hL = 0.5 * R.box, rc2 = A.rc * A.rc, dt = A.dt;
   const long long lbase = (long long)off * A.lstride;
   double esum = 0.0, vir = 0.0, ek = 0.0;
-  for (int i = tid; i < N; i += NT) {
+  if (MIXED && A.lg > 0) {
+    // 1 << lg consecutive lanes per atom (rows of a liquid droplet run to
+    // ~130 entries): lane `sub` of the group takes entries sub, sub + G, ...
+    // with its own Kahan sums; the group then merges them in a fixed tree
+    // (xor shuffles), so the result is deterministic for a given G.  The
+    // loop is warp-uniform (32 / G atoms per warp and pass) so that every
+    // lane takes part in the shuffles.
+    const int lg = A.lg, G = 1 << lg, lane = tid & 31, sub = tid & (G - 1);
+    for (int w0 = (gt - lane) >> lg; w0 < N; w0 += GT >> lg) {
+      const int i = w0 + (lane >> lg);
+      const bool own = i < N;
+      const int ii = own ? i : w0;
+      const double xi = P.x(ii), yi = P.y(ii), zi = P.z(ii);
+      const int len = own ? A.rlen[off + i] : 0;
+      float fx = 0.f, fy = 0.f, fz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+      const int* lp = A.list + lbase + (long long)sub * N + ii;
+      const long long step = (long long)G * N;
+      for (int k = sub; k < len; k += G, lp += step) {
+        const int j = *lp;
+        double dx = mi_sel(xi - P.x(j), L, hL);
+        double dy = mi_sel(yi - P.y(j), L, hL);
+        double dz = mi_sel(zi - P.z(j), L, hL);
+        double r2d = dx * dx + dy * dy + dz * dz;
+        if (r2d <= rc2) {
+          float r2 = (float)r2d;
+          float ri2 = clmd_rcp_f32(r2);
+          float r6 = ri2 * ri2 * ri2;
+          float fij = 48.0f * ri2 * r6 * (r6 - 0.5f);
+          kahan(fx, cx, fij * (float)dx);
+          kahan(fy, cy, fij * (float)dy);
+          kahan(fz, cz, fij * (float)dz);
+          if (energies && i < j) {
+            esum += (double)(4.0f * r6 * (r6 - 1.0f));
+            vir += (double)(fij * r2);
+          }
+        }
+      }
+      for (int o = 1; o < G; o <<= 1) {  // each partner's compensated sum
+        const float px = __shfl_xor_sync(0xffffffffu, __fsub_rn(fx, cx), o);
+        const float py = __shfl_xor_sync(0xffffffffu, __fsub_rn(fy, cy), o);
+        const float pz = __shfl_xor_sync(0xffffffffu, __fsub_rn(fz, cz), o);
+        kahan(fx, cx, px);
+        kahan(fy, cy, py);
+        kahan(fz, cz, pz);
+      }
+      if (!own || sub != 0) continue;
+      float* a = (float*)A.a;
+      a[off + i] = fx;
+      a[A.pool + off + i] = fy;
+      a[2 * A.pool + off + i] = fz;
+      const double ax = (double)fx, ay = (double)fy, az = (double)fz;
+      if (NHF) {
+        const double dth = 0.5 * dt;
+        const double wx = A.vx[off + i] + dth * ax;
+        const double wy = A.vy[off + i] + dth * ay;
+        const double wz = A.vz[off + i] + dth * az;
+        A.vxn[off + i] = wx;
+        A.vyn[off + i] = wy;
+        A.vzn[off + i] = wz;
+        *s0 += wx * wx + wy * wy + wz * wz;
+      }
+      if (kick) {
+        double vxi = A.vx[off + i] + 0.5 * ax * dt;
+        double vyi = A.vy[off + i] + 0.5 * ay * dt;
+        double vzi = A.vz[off + i] + 0.5 * az * dt;
+        A.vx[off + i] = vxi;
+        A.vy[off + i] = vyi;
+        A.vz[off + i] = vzi;
+        if (energies) ek += 0.5 * (vxi * vxi + vyi * vyi + vzi * vzi);
+      }
+    }
+  } else
+  for (int i = gt; i < N; i += GT) {
     const double xi = P.x(i), yi = P.y(i), zi = P.z(i);
     const int len = A.rlen[off + i];
     double ax, ay, az;
@@ -673,16 +907,16 @@ __device__ void forces(Rep& R, Cta& C, const Args& A, const Pos<SM>& P, bool kic
     }
   }
   if (energies) {
-    double e = cta_sum<NT>(esum, C.red);
-    double w = cta_sum<NT>(vir, C.red);
-    double k = kick ? cta_sum<NT>(ek, C.red) : 0.0;
+    double e = grp_sum<NT, CS>(esum, C);
+    double w = grp_sum<NT, CS>(vir, C);
+    double k = kick ? grp_sum<NT, CS>(ek, C) : 0.0;
     if (tid == 0) {
       R.epot = e;
       R.virial = w;
       if (kick) R.ekin = k;
     }
   }
-  __syncthreads();
+  gsync<CS>();
 }
 
 template <bool MIXED>
@@ -701,36 +935,38 @@ __device__ __forceinline__ void get_a(const Args& A, int k, double& ax, double& 
 }
 
 // stopdead-m.f:28-69 (one species, m = 1): COM removal and rescale to T
-template <int NT>
+template <int NT, int CS>
 __device__ void stopdead(Rep& R, Cta& C, const Args& A) {
   const int N = R.natom, off = R.off, tid = threadIdx.x;
+  const int gt = gtid<NT, CS>();
+  constexpr int GT = NT * CS;
   for (int loop = 0; loop < 10; loop++) {
     double px = 0, py = 0, pz = 0;
-    for (int i = tid; i < N; i += NT) {
+    for (int i = gt; i < N; i += GT) {
       px += A.vx[off + i];
       py += A.vy[off + i];
       pz += A.vz[off + i];
     }
-    double vxs = cta_sum<NT>(px, C.red) / (double)N;
-    double vys = cta_sum<NT>(py, C.red) / (double)N;
-    double vzs = cta_sum<NT>(pz, C.red) / (double)N;
+    double vxs = grp_sum<NT, CS>(px, C) / (double)N;
+    double vys = grp_sum<NT, CS>(py, C) / (double)N;
+    double vzs = grp_sum<NT, CS>(pz, C) / (double)N;
     double ek = 0.0;
-    for (int i = tid; i < N; i += NT) {
+    for (int i = gt; i < N; i += GT) {
       double a = A.vx[off + i] - vxs, b = A.vy[off + i] - vys, c = A.vz[off + i] - vzs;
       A.vx[off + i] = a;
       A.vy[off + i] = b;
       A.vz[off + i] = c;
       ek += 0.5 * (a * a + b * b + c * c);
     }
-    ek = cta_sum<NT>(ek, C.red);
+    ek = grp_sum<NT, CS>(ek, C);
     double kf = sqrt(R.ekinT / ek);  // scalev-nh-m.f with step = -1
-    for (int i = tid; i < N; i += NT) {
+    for (int i = gt; i < N; i += GT) {
       A.vx[off + i] *= kf;
       A.vy[off + i] *= kf;
       A.vz[off + i] *= kf;
     }
     if (tid == 0) R.ekin = R.ekinT;
-    __syncthreads();
+    gsync<CS>();
   }
 }
 
@@ -758,20 +994,22 @@ __device__ __forceinline__ void uunion(int* par, int a, int b) {
 }
 
 // stoddard-pbc-n-m.f (one species) + chk-nucleation.f at step `step`
-template <int NT, bool SM>
+template <int NT, bool SM, int CS>
 __device__ void analysis(Rep& R, Cta& C, const Args& A, const Pos<SM>& P, int step) {
   const int N = R.natom, off = R.off, tid = threadIdx.x;
+  const int gt = gtid<NT, CS>();
+  constexpr int GT = NT * CS;
   int* par = A.parent + off;
   int* cs = A.cs + off;
-  for (int i = tid; i < N; i += NT) {
+  for (int i = gt; i < N; i += GT) {
     par[i] = i;
     cs[i] = 0;
   }
-  __syncthreads();
+  gsync<CS>();
   const double L = R.box, iL = R.ibox, rc2 = A.atskin * A.atskin;
   const double bf1 = (double)(int)(R.atrskin) + 2.0, bf2 = bf1 + 0.5;
   const long long lbase = (long long)off * A.lstride;
-  for (int i = tid; i < N - 1; i += NT) {
+  for (int i = gt; i < N - 1; i += GT) {
     const double xi = P.x(i), yi = P.y(i), zi = P.z(i);
     const int len = A.rlen[off + i];
     for (int k = 0; k < len; k++) {
@@ -784,38 +1022,39 @@ __device__ void analysis(Rep& R, Cta& C, const Args& A, const Pos<SM>& P, int st
       if (r2 <= rc2) uunion(par, i, j);
     }
   }
-  __syncthreads();
+  gsync<CS>();
   if (R.reorder) {
     // slots are in cell order: a cluster's label is the smallest atom number
     // (orig) among its slots, as for atoms kept in their own order.  sorted[]
     // is free outside the rebuild.
     int* mo = A.sorted + off;
-    for (int i = tid; i < N; i += NT) mo[i] = 0x7fffffff;
-    __syncthreads();
-    for (int i = tid; i < N; i += NT) atomicMin(mo + ufind(par, i), A.orig[off + i] - off);
-    __syncthreads();
-    for (int i = tid; i < N; i += NT) {
+    for (int i = gt; i < N; i += GT) mo[i] = 0x7fffffff;
+    gsync<CS>();
+    for (int i = gt; i < N; i += GT) atomicMin(mo + ufind(par, i), A.orig[off + i] - off);
+    gsync<CS>();
+    for (int i = gt; i < N; i += GT) {
       int r = ufind(par, i);
       A.cl[A.orig[off + i]] = mo[r] + 1;  // by atom number: slots move at rebuilds
       atomicAdd(cs + r, 1);
     }
   } else {
-    for (int i = tid; i < N; i += NT) {
+    for (int i = gt; i < N; i += GT) {
       int r = ufind(par, i);
       A.cl[off + i] = r + 1;
       atomicAdd(cs + r, 1);
     }
   }
-  __syncthreads();
+  gsync<CS>();
   double m = 0.0;
-  for (int i = tid; i < N; i += NT) m = fmax(m, (double)cs[i]);
-  int maxcs = (int)cta_max<NT>(m, C.red);
+  for (int i = gt; i < N; i += GT) m = fmax(m, (double)cs[i]);
+  int maxcs = (int)grp_max<NT, CS>(m, C);
   if (tid == 0) {
     R.maxcs = maxcs;
     R.cstep = step;
     // first step at which the largest cluster reached each size
     int* fpt = A.fpt + (size_t)C.rep * kFptCap;
-    for (int s = R.fpt_top + 1; s <= maxcs && s <= kFptCap; s++) fpt[s - 1] = step;
+    if (grank<CS>() == 0)
+      for (int s = R.fpt_top + 1; s <= maxcs && s <= kFptCap; s++) fpt[s - 1] = step;
     if (maxcs > R.fpt_top) R.fpt_top = maxcs;
     // chk-nucleation.f:33-56
     int tim = (maxcs >= R.csover && R.csover <= N) ? step : 0;
@@ -828,15 +1067,17 @@ __device__ void analysis(Rep& R, Cta& C, const Args& A, const Pos<SM>& P, int st
       R.clbrkt = 0;
     }
   }
-  __syncthreads();
+  gsync<CS>();
 }
 
 // ---------------------------------------------------------------------------
 // one replica, one window
 // ---------------------------------------------------------------------------
-template <int NT, bool SM, bool MIXED>
+template <int NT, bool SM, bool MIXED, int CS>
 __device__ void run_window(Rep& R, Cta& C, const Args& A) {
   const int tid = threadIdx.x;
+  const int gt = gtid<NT, CS>();
+  constexpr int GT = NT * CS;
   const int N = R.natom, off = R.off;
   const bool nh = A.integrator == CLMD_INT_NOSE;
   const double dt = A.dt;
@@ -844,12 +1085,12 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
   bool vin_n = false;  // uniform: the current velocities are in vxn, not vx
   double vsc = 1.0;    // mixed: the velocities are vn * vsc (clmd_nh_root)
   if (SM) {
-    for (int i = tid; i < N; i += NT) {
+    for (int i = gt; i < N; i += GT) {
       C.sx[i] = A.x[off + i];
       C.sy[i] = A.y[off + i];
       C.sz[i] = A.z[off + i];
     }
-    __syncthreads();
+    gsync<CS>();
   }
   // the grid of the current list
   if (tid == 0) {
@@ -864,14 +1105,14 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
     C.offx[1] = n >= 3 ? 0 : 1;
     C.offx[2] = 1;
   }
-  __syncthreads();
+  gsync<CS>();
   if (!R.started) {
     // stopdead(-1), neighbor(0), a = 0 + AccAtom, main.f:156-166
-    stopdead<NT>(R, C, A);
+    stopdead<NT, CS>(R, C, A);
     if (tid == 0) C.flag = prologue(R, C, A, 0);
-    __syncthreads();
-    if (!C.flag || !rebuild<NT, SM>(R, C, A, P)) goto out;
-    forces<NT, SM, MIXED>(R, C, A, P, false, true);
+    gsync<CS>();
+    if (!C.flag || !rebuild<NT, SM, CS>(R, C, A, P)) goto out;
+    forces<NT, SM, MIXED, CS>(R, C, A, P, false, true);
     if (tid == 0) {
       R.sumv2 = 2.0 * R.ekin;
       R.psi = (R.ethst == 'N') ? (R.sumv2 - R.nkt3_d) / R.Q : 0.0;
@@ -879,7 +1120,7 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
       R.started = 1;
       R.cstep = -1;
     }
-    __syncthreads();
+    gsync<CS>();
   }
   // C.nsteps MD steps in this launch; the analysis and chk_nucleation run
   // whenever the step counter reaches a multiple of ftcsi (wrt-csi.f:27,
@@ -888,21 +1129,21 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
     if (R.done || R.status) break;
     if (A.ftcsi > 0 && R.step % A.ftcsi == 0 && R.cstep != R.step) {
       if (vin_n) {  // velocities back in vx for the analysis
-        for (int i = tid; i < N; i += NT) {
+        for (int i = gt; i < N; i += GT) {
           A.vx[off + i] = MIXED ? A.vxn[off + i] * vsc : A.vxn[off + i];
           A.vy[off + i] = MIXED ? A.vyn[off + i] * vsc : A.vyn[off + i];
           A.vz[off + i] = MIXED ? A.vzn[off + i] * vsc : A.vzn[off + i];
         }
         vin_n = false;
-        __syncthreads();
+        gsync<CS>();
       }
-      analysis<NT, SM>(R, C, A, P, R.step);
+      analysis<NT, SM, CS>(R, C, A, P, R.step);
       if (R.done) break;
     }
     if (R.step >= R.budget) {
-      __syncthreads();
+      gsync<CS>();
       if (tid == 0) R.done = 2;
-      __syncthreads();
+      gsync<CS>();
       break;
     }
     {
@@ -917,7 +1158,7 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
       const double* svz = vin_n ? A.vzn : A.vz;
       const double sc = vin_n ? vsc : 1.0;
       vin_n = false;
-      for (int i = tid; i < N; i += NT) {
+      for (int i = gt; i < N; i += GT) {
         double vxi = svx[off + i], vyi = svy[off + i], vzi = svz[off + i];
         if (MIXED) {
           vxi = vxi * sc;
@@ -950,7 +1191,7 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
         A.vz[off + i] = vzi;
         d2 = fmax(d2, dx * dx + dy * dy + dz * dz);
       }
-      cta_maxsum<NT>(d2, sv, C.red);
+      grp_maxsum<NT, CS>(d2, sv, C);
       const double dmmr = d2, sumv2 = sv;
       if (tid == 0) {
         if (nh) {
@@ -963,11 +1204,11 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
         C.flag = 1;
         if (skin(R, A, dmmr)) C.flag = prologue(R, C, A, step) ? 2 : 0;
       }
-      __syncthreads();
+      gsync<CS>();
       if (C.flag == 0) goto out;
-      if (C.flag == 2 && !rebuild<NT, SM>(R, C, A, P)) goto out;
+      if (C.flag == 2 && !rebuild<NT, SM, CS>(R, C, A, P)) goto out;
       if (!nh) {
-        forces<NT, SM, MIXED>(R, C, A, P, true, last);
+        forces<NT, SM, MIXED, CS>(R, C, A, P, true, last);
       } else {
         // int-verlet-nh-mav.f:91-180 with block reductions.  Each sweep is one
         // pass: it updates vn from this sweep's delps and accumulates the
@@ -976,10 +1217,10 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
         const double Q = R.Q, err = 1.0e-10, psi1 = R.psi, dtQ = dt / Q;
         if (MIXED) {
           double S = 0.0, unused = 0.0, p;
-          forces<NT, SM, MIXED, true>(R, C, A, P, false, last, psi1, dtQ, &S, &unused);
-          if (!cta_nh_root<NT>(S, psi1, R.nkt3_i, dth, Q, C.red, S, p)) {
+          forces<NT, SM, MIXED, CS, true>(R, C, A, P, false, last, psi1, dtQ, &S, &unused);
+          if (!grp_nh_root<NT, CS>(S, psi1, R.nkt3_i, dth, Q, C, S, p)) {
             if (tid == 0 && R.status == 0) R.status = CLMD_ERR_NH_NOCONVERGE;
-            __syncthreads();
+            gsync<CS>();
             goto out;
           }
           vsc = 1.0 / (1.0 + dth * p);
@@ -991,9 +1232,9 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
           }
         } else {
           double sumv2n = 0.0, dpsum = 0.0;
-          forces<NT, SM, MIXED, true>(R, C, A, P, false, last, psi1, dtQ, &sumv2n, &dpsum);
+          forces<NT, SM, MIXED, CS, true>(R, C, A, P, false, last, psi1, dtQ, &sumv2n, &dpsum);
           int nr0 = 0;
-          cta_sum2<NT>(sumv2n, dpsum, nr0, C.red);
+          grp_sum2<NT, CS>(sumv2n, dpsum, nr0, C);
           double psn = psi1;
           int ready = 0;
           for (int iter = 1; iter <= 1000; iter++) {
@@ -1005,7 +1246,7 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
             const double rdi = 1.0 / di;
             double s2 = 0.0, dpn = 0.0;
             int nr = 0;
-            for (int i = tid; i < N; i += NT) {
+            for (int i = gt; i < N; i += GT) {
               double ax, ay, az;
               get_a<MIXED>(A, off + i, ax, ay, az);
               const double V[3] = {A.vx[off + i], A.vy[off + i], A.vz[off + i]};
@@ -1031,7 +1272,7 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
             }
             sumv2n = s2;
             dpsum = dpn;
-            cta_sum2<NT>(sumv2n, dpsum, nr, C.red);
+            grp_sum2<NT, CS>(sumv2n, dpsum, nr, C);
             if (!nr) {
               ready = 1;
               break;
@@ -1039,7 +1280,7 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
           }
           if (!ready) {
             if (tid == 0 && R.status == 0) R.status = CLMD_ERR_NH_NOCONVERGE;
-            __syncthreads();
+            gsync<CS>();
             goto out;
           }
           vin_n = true;  // the step's velocities are in vxn until the next drift
@@ -1051,45 +1292,45 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
         }
       }
       if (tid == 0) R.step = step + 1;
-      __syncthreads();
+      gsync<CS>();
     }
     // a spent budget ends the replica at once, after the analysis due at its
     // last step, rather than at the start of the next launch
     if (R.step >= R.budget) {
       if (vin_n) {
-        for (int i = tid; i < N; i += NT) {
+        for (int i = gt; i < N; i += GT) {
           A.vx[off + i] = MIXED ? A.vxn[off + i] * vsc : A.vxn[off + i];
           A.vy[off + i] = MIXED ? A.vyn[off + i] * vsc : A.vyn[off + i];
           A.vz[off + i] = MIXED ? A.vzn[off + i] * vsc : A.vzn[off + i];
         }
         vin_n = false;
-        __syncthreads();
+        gsync<CS>();
       }
       if (A.ftcsi > 0 && R.step % A.ftcsi == 0 && R.cstep != R.step)
-        analysis<NT, SM>(R, C, A, P, R.step);
-      __syncthreads();
+        analysis<NT, SM, CS>(R, C, A, P, R.step);
+      gsync<CS>();
       if (tid == 0 && !R.done) R.done = 2;
-      __syncthreads();
+      gsync<CS>();
       break;
     }
   }
 out:
-  __syncthreads();
+  gsync<CS>();
   if (vin_n) {
-    for (int i = tid; i < N; i += NT) {
+    for (int i = gt; i < N; i += GT) {
       A.vx[off + i] = MIXED ? A.vxn[off + i] * vsc : A.vxn[off + i];
       A.vy[off + i] = MIXED ? A.vyn[off + i] * vsc : A.vyn[off + i];
       A.vz[off + i] = MIXED ? A.vzn[off + i] * vsc : A.vzn[off + i];
     }
   }
   if (SM) {
-    for (int i = tid; i < N; i += NT) {
+    for (int i = gt; i < N; i += GT) {
       A.x[off + i] = C.sx[i];
       A.y[off + i] = C.sy[i];
       A.z[off + i] = C.sz[i];
     }
   }
-  __syncthreads();
+  gsync<CS>();
 }
 
 // MINB: CTAs per SM the register budget must allow -- 512 / NT (<= 128
@@ -1131,7 +1372,7 @@ __global__ void __launch_bounds__(NT, MINB) k_ens(Args A) {
       asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
     }
     __syncthreads();
-    if (!R.done && !R.status) run_window<NT, SM, MIXED>(R, C, A);
+    if (!R.done && !R.status) run_window<NT, SM, MIXED, 1>(R, C, A);
     if (threadIdx.x == 0 && R.step > step0) {
       unsigned long long t1;
       asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
@@ -1144,6 +1385,62 @@ __global__ void __launch_bounds__(NT, MINB) k_ens(Args A) {
     }
     if (threadIdx.x == 0) A.summary[r] = make_int4(R.done, R.status, R.step, R.maxcs);
     __syncthreads();
+  }
+}
+
+// A replica too large for one SM's shared memory on a thread-block cluster
+// of CS CTAs (one per SM): positions in global memory, the per-atom loops
+// split over the cluster's CS * NT threads, the replica-wide barriers and
+// reductions cluster-wide (see grp_*).  Every CTA keeps its own copy of the
+// replica record and cell starts and applies the same scalar logic to the
+// same totals; rank 0 alone writes the shared results back.  Each cluster
+// takes replicas from the device counter like the single-CTA kernel.
+template <int NT, bool MIXED, int CS>
+__global__ void __launch_bounds__(NT, 1) k_ens_cl(Args A) {
+  extern __shared__ double dsm[];
+  __shared__ Rep R;
+  __shared__ Cta C;
+  __shared__ int item;
+  auto cl = cg::this_cluster();
+  const unsigned rank = cl.block_rank();
+  for (;;) {
+    if (rank == 0 && threadIdx.x == 0) item = atomicAdd(A.ctr, 1);
+    cl.sync();
+    const int it = *cl.map_shared_rank(&item, 0);
+    cl.sync();  // rank 0's item is read by all before any CTA claims again or exits
+    if (it >= A.nitems) break;
+    const int r = A.items[it];
+    {
+      const int* src = (const int*)(A.reps + r);
+      int* dst = (int*)&R;
+      for (int k = threadIdx.x; k < (int)(sizeof(Rep) / 4); k += NT) dst[k] = src[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      C.rep = r;
+      C.cstart = (int*)dsm;
+      C.sx = C.sy = C.sz = nullptr;
+    }
+    unsigned long long t0 = 0;
+    const int step0 = R.step;
+    if (threadIdx.x == 0) {
+      C.nsteps = A.iwin ? A.iwin[it] : A.nwin * (A.ftcsi > 0 ? A.ftcsi : 1);
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    }
+    cl.sync();
+    if (!R.done && !R.status) run_window<NT, false, MIXED, CS>(R, C, A);
+    if (rank == 0) {
+      if (threadIdx.x == 0 && R.step > step0) {
+        unsigned long long t1;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
+        A.wtime[r] = (float)((double)(t1 - t0) * 1e-6 / (double)(R.step - step0));
+      }
+      const int* src = (const int*)&R;
+      int* dst = (int*)(A.reps + r);
+      for (int k = threadIdx.x; k < (int)(sizeof(Rep) / 4); k += NT) dst[k] = src[k];
+      if (threadIdx.x == 0) A.summary[r] = make_int4(R.done, R.status, R.step, R.maxcs);
+    }
+    cl.sync();
   }
 }
 
@@ -1176,11 +1473,20 @@ struct clmd_ensemble {
   double* d_stage = nullptr;  // bulk copies in atom order (pool doubles, on first use)
   int4* h_summary = nullptr;  // pinned copy of A.summary
   bool reps_stale = false;    // h_reps older than the device records
-  // size classes: each has its own block size, shared-memory budget, stream
-  static constexpr int kClasses = 4;
-  int cls_max[kClasses] = {2048, 4096, 6144, 1 << 30};  // measured best of a few splits
+  // size classes: each has its own block size, shared-memory budget, stream.
+  // 0-3: one CTA per replica, split by atom count (cls_max); 4-7: replicas
+  // whose positions do not fit in shared memory, one thread-block cluster
+  // of 2, 4, 8 or 16 CTAs per replica (kClusterAtoms atoms per CTA or more)
+  static constexpr int kClasses = 8;
+  static constexpr int kCtaClasses = 4;
+  int cls_max[kCtaClasses] = {2048, 4096, 6144, 1 << 30};  // measured best of a few splits
   // the shapes the autotuner picks on the batched workload (used until it runs)
-  int cls_threads[kClasses] = {512 | CLMD_ENS_LEAN, 1024, 1024, 1024};
+  int cls_threads[kClasses] = {512 | CLMD_ENS_LEAN, 1024, 1024, 1024, 1024, 1024, 1024, 1024};
+  int cls_cs[kClasses] = {1, 1, 1, 1, 2, 4, 8, 16};
+  int cls_lg[kClasses] = {};  // mixed force pass: 1 << lg lanes per atom
+  int cl_max_clusters[kClasses] = {};  // co-resident clusters per launch (0: size unusable)
+  int cl_region0[kClasses] = {};       // first cell-count region of each cluster class
+  bool use_clusters = true;
   cudaStream_t cstream[kClasses] = {};
   cudaEvent_t ev0[kClasses] = {}, ev1[kClasses] = {}, evj = nullptr;
   cudaEvent_t evdone[kClasses] = {};  // join of each class stream
@@ -1230,6 +1536,9 @@ static int cells_for(size_t cap, int nmax, bool* sm) {
 
 // the block shapes k_ens is compiled for (0: autotune)
 static bool shape_ok(int shape) {
+  const int lanes = (shape >> CLMD_ENS_LANES_SHIFT) & 0xff;
+  if (lanes > 2) return false;
+  shape &= ~(0xff << CLMD_ENS_LANES_SHIFT);
   switch (shape) {
     case 0: case 128: case 256: case 512: case 1024:
     case 128 | CLMD_ENS_LEAN: case 256 | CLMD_ENS_LEAN: case 512 | CLMD_ENS_LEAN:
@@ -1237,6 +1546,67 @@ static bool shape_ok(int shape) {
     default:
       return false;
   }
+}
+
+typedef void (*EnsKernel)(Args);
+
+// the cluster kernel of cs CTAs per replica (1024 threads each)
+static EnsKernel cluster_kernel(int cs, bool mixed) {
+  switch (cs) {
+    case 2: return mixed ? k_ens_cl<1024, true, 2> : k_ens_cl<1024, false, 2>;
+    case 4: return mixed ? k_ens_cl<1024, true, 4> : k_ens_cl<1024, false, 4>;
+    case 8: return mixed ? k_ens_cl<1024, true, 8> : k_ens_cl<1024, false, 8>;
+    default: return mixed ? k_ens_cl<1024, true, 16> : k_ens_cl<1024, false, 16>;
+  }
+}
+static size_t cluster_smem(int ncmax) {
+  return sizeof(int) * (((size_t)ncmax * ncmax * ncmax + 2 + 1) & ~(size_t)1);
+}
+
+// how many clusters of each size can be resident at once (0: that size
+// cannot be launched here, e.g. 16 without non-portable cluster support),
+// and each class's share of the cell-count regions
+static int setup_clusters(clmd_ensemble* E) {
+  const bool mixed = E->cfg.precision == CLMD_PREC_MIXED;
+  const size_t smem = cluster_smem(kNcMax);
+  int region = 0;
+  for (int c = clmd_ensemble::kCtaClasses; c < clmd_ensemble::kClasses; c++) {
+    const int cs = E->cls_cs[c];
+    EnsKernel k = cluster_kernel(cs, mixed);
+    E->cl_max_clusters[c] = 0;
+    if (cs > 8 && cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                      cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    E->attr_smem[(void*)k] = smem;
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(cs);
+    lc.blockDim = dim3(1024);
+    lc.dynamicSmemBytes = smem;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, (void*)k, &lc) != cudaSuccess) {
+      cudaGetLastError();
+      n = 0;
+    }
+    n = std::min(n, E->nsm / cs);  // regions: the classes' shares sum to < nsm
+    E->cl_max_clusters[c] = n;
+    E->cl_region0[c] = region;
+    region += E->nsm / cs;
+  }
+  return CLMD_OK;
 }
 
 extern "C" int clmd_ens_create(const clmd_ens_config* cfg, clmd_ensemble** out) {
@@ -1267,12 +1637,16 @@ extern "C" int clmd_ens_create(const clmd_ens_config* cfg, clmd_ensemble** out) 
     ECK(cudaEventCreate(&E->ev0[c]));
     ECK(cudaEventCreate(&E->ev1[c]));
     ECK(cudaEventCreateWithFlags(&E->evdone[c], cudaEventDisableTiming));
-    if (cfg->threads > 0) E->cls_threads[c] = cfg->threads;
+    if (cfg->threads > 0 && c < clmd_ensemble::kCtaClasses) E->cls_threads[c] = cfg->threads;
   }
   ECK(cudaEventCreateWithFlags(&E->evj, cudaEventDisableTiming));
   {
     const char* g = getenv("CLMD_ENS_GRAPHS");
     E->use_graphs = !(g && g[0] == '0');
+    // CLMD_ENS_CLUSTERS=0: replicas too large for shared memory run on one
+    // CTA each (class 3) instead of on a thread-block cluster
+    const char* k = getenv("CLMD_ENS_CLUSTERS");
+    E->use_clusters = !(k && k[0] == '0');
     // CLMD_ENS_CLASSES="a,b,c": upper atom counts of the first three size
     // classes (ascending), for tuning the split
     const char* cs = getenv("CLMD_ENS_CLASSES");
@@ -1312,6 +1686,13 @@ extern "C" int clmd_ens_create(const clmd_ens_config* cfg, clmd_ensemble** out) 
   ECK(cudaMalloc(&E->d_iwin, sizeof(int) * R));
   ECK(cudaMallocHost(&E->h_iwin, sizeof(int) * R));
   ECK(cudaMalloc(&A.wtime, sizeof(float) * R));
+  // cell counts of the cluster classes: one region per co-resident cluster
+  A.cscr_stride = (long long)kNcMax * kNcMax * kNcMax + 2;
+  ECK(cudaMalloc(&A.cscr, sizeof(int) * A.cscr_stride * (long long)E->nsm));
+  {
+    int st = setup_clusters(E);
+    if (st) return st;
+  }
   ECK(cudaMemset(A.wtime, 0, sizeof(float) * R));
   ECK(cudaMallocHost(&E->h_wtime, sizeof(float) * R));
   memset(E->h_wtime, 0, sizeof(float) * R);
@@ -1339,7 +1720,7 @@ extern "C" int clmd_ens_destroy(clmd_ensemble* E) {
   Args& A = E->A;
   void* ps[] = {A.x, A.y, A.z, A.vx, A.vy, A.vz, A.vxn, A.vyn, A.vzn, A.a, A.list, A.rlen,
                 A.sorted, A.cellid, A.parent, A.cs, A.cl, A.orig, A.reps, A.fpt, A.summary,
-                E->d_items, E->d_ctr, E->d_iwin, A.wtime, E->d_stage};
+                E->d_items, E->d_ctr, E->d_iwin, A.wtime, E->d_stage, A.cscr};
   for (void* p : ps)
     if (p) cudaFree(p);
   if (E->h_reps) cudaFreeHost(E->h_reps);
@@ -1491,8 +1872,6 @@ extern "C" int clmd_ens_remove(clmd_ensemble* E, int32_t slot) {
   return CLMD_OK;
 }
 
-typedef void (*EnsKernel)(Args);
-
 template <int NT, int MINB>
 static EnsKernel pick(bool sm, bool mixed) {
   if (sm) return mixed ? k_ens<NT, true, true, MINB> : k_ens<NT, true, false, MINB>;
@@ -1502,6 +1881,7 @@ static EnsKernel pick(bool sm, bool mixed) {
 // a block shape: threads per CTA, with CLMD_ENS_LEAN for the 64-register
 // variant (128, 256 and 512 threads)
 static int shape_threads(int shape) { return shape & 0xffff; }
+static int shape_lanes_log2(int shape) { return (shape >> CLMD_ENS_LANES_SHIFT) & 3; }
 
 static EnsKernel kernel_for(int shape, bool sm, bool mixed) {
   const bool lean = (shape & CLMD_ENS_LEAN) != 0;
@@ -1518,10 +1898,13 @@ struct ClassLaunch {
   EnsKernel k = nullptr;
   size_t smem = 0;
   int grid = 0, nt = 0, ncmax = 1, item0 = 0, nitems = 0;
+  int cs = 1;       // CTAs per replica (thread-block cluster size)
+  int lg = 0;       // lanes per atom in the mixed force pass: 1 << lg
+  int region0 = 0;  // first cell-count region (cluster classes)
 };
 
-static int prepare_class(clmd_ensemble* E, int item0, int nitems, const int* slots, int shape,
-                         ClassLaunch& L) {
+static int prepare_class(clmd_ensemble* E, int c, int item0, int nitems, const int* slots,
+                         int shape, ClassLaunch& L) {
   L = ClassLaunch();
   L.item0 = item0;
   L.nitems = nitems;
@@ -1529,6 +1912,21 @@ static int prepare_class(clmd_ensemble* E, int item0, int nitems, const int* slo
   L.nt = nt;
   if (nitems == 0) return CLMD_OK;
   const bool mixed = E->cfg.precision == CLMD_PREC_MIXED;
+  L.lg = mixed ? shape_lanes_log2(shape) : 0;
+  if (c >= clmd_ensemble::kCtaClasses) {
+    // one thread-block cluster per replica: 1024 threads per CTA, the cell
+    // starts (kNcMax^3 at most) in each CTA's shared memory
+    L.cs = E->cls_cs[c];
+    L.nt = 1024;
+    L.k = cluster_kernel(L.cs, mixed);
+    for (int k = 0; k < nitems; k++) L.ncmax = std::max(L.ncmax, E->h_reps[slots[k]].ncmax);
+    L.smem = cluster_smem(L.ncmax);
+    L.region0 = E->cl_region0[c];
+    const int nclu = std::min(E->cl_max_clusters[c], nitems);
+    if (nclu < 1) return CLMD_ERR_ARG;
+    L.grid = nclu * L.cs;
+    return CLMD_OK;
+  }
   // positions stay in shared memory if every replica of the class fits
   bool sm = true;
   for (int k = 0; k < nitems; k++) {
@@ -1568,9 +1966,27 @@ static int enqueue_class(clmd_ensemble* E, int c, const ClassLaunch& L, int nwin
   A.nitems = L.nitems;
   A.nwin = nwin;
   A.ncmax = L.ncmax;
+  A.lg = L.lg;
   const unsigned fl = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
   ECK(cudaEventRecordWithFlags(E->ev0[c], st, fl));
-  L.k<<<L.grid, L.nt, L.smem, st>>>(A);
+  if (L.cs > 1) {
+    A.cscr = E->A.cscr + (long long)L.region0 * E->A.cscr_stride;
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(L.grid);
+    lc.blockDim = dim3(L.nt);
+    lc.dynamicSmemBytes = L.smem;
+    lc.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = L.cs;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    ECK(cudaLaunchKernelEx(&lc, L.k, A));
+  } else {
+    L.k<<<L.grid, L.nt, L.smem, st>>>(A);
+  }
   ECK(cudaGetLastError());
   ECK(cudaEventRecordWithFlags(E->ev1[c], st, fl));
   ECK(cudaEventRecord(E->evdone[c], st));
@@ -1584,14 +2000,31 @@ static int enqueue_class(clmd_ensemble* E, int c, const ClassLaunch& L, int nwin
 // that every CTA stays busy about min_ms whatever its replica's size (a
 // replica not yet timed runs a few steps)
 // only >= 0: that size class alone (the autotuner's trials)
+// the cluster class of a replica whose positions do not fit in shared
+// memory: about kClusterAtoms atoms or more per CTA, the cluster size a power
+// of two in [2, 16], the largest usable one not above it (-1: none usable)
+constexpr int kClusterAtoms = 3072;
+static int cluster_class(const clmd_ensemble* E, int n) {
+  int want = 2;
+  while (want < 16 && want * kClusterAtoms < n) want *= 2;
+  for (int c = clmd_ensemble::kClasses - 1; c >= clmd_ensemble::kCtaClasses; c--)
+    if (E->cls_cs[c] <= want && E->cl_max_clusters[c] > 0) return c;
+  return -1;
+}
+
 static int launch_all(clmd_ensemble* E, int nwin, const int* threads, float min_ms = 0.0f,
                       int only = -1) {
   std::vector<int> cls[clmd_ensemble::kClasses];
   int nmax[clmd_ensemble::kClasses] = {};
   for (int s = 0; s < E->cfg.max_replicas; s++)
     if (E->used[s] && !E->h_summary[s].x && !E->h_summary[s].y) {
-      int n = E->h_reps[s].natom, c = 0;
-      while (c < clmd_ensemble::kClasses - 1 && n > E->cls_max[c]) c++;
+      const int n = E->h_reps[s].natom;
+      int c = -1;
+      if (E->use_clusters && E->h_reps[s].reorder == 1) c = cluster_class(E, n);
+      if (c < 0) {
+        c = 0;
+        while (c < clmd_ensemble::kCtaClasses - 1 && n > E->cls_max[c]) c++;
+      }
       if (only >= 0 && c != only) continue;
       cls[c].push_back(s);
       nmax[c] = std::max(nmax[c], n);
@@ -1633,9 +2066,10 @@ static int launch_all(clmd_ensemble* E, int nwin, const int* threads, float min_
     int off = 0;
     for (int c = 0; c < clmd_ensemble::kClasses; c++) {
       for (int s : cls[c]) E->last_atoms[c] += E->h_reps[s].natom;
-      int st = prepare_class(E, off, (int)cls[c].size(), cls[c].data(), threads[c], L[c]);
+      int st = prepare_class(E, c, off, (int)cls[c].size(), cls[c].data(), threads[c], L[c]);
       if (st) return st;
       key.push_back(L[c].nt);
+      key.push_back(L[c].lg);
       key.push_back(L[c].grid);
       key.push_back((long long)L[c].smem);
       key.push_back((long long)(size_t)L[c].k);
@@ -1651,7 +2085,8 @@ static int launch_all(clmd_ensemble* E, int nwin, const int* threads, float min_
     ECK(cudaMemcpyAsync(E->d_items, E->h_items, sizeof(int) * total, cudaMemcpyHostToDevice,
                         E->stream));
     ECK(cudaEventRecord(E->evj, E->stream));
-    for (int c = 0; c < clmd_ensemble::kClasses; c++) {
+    // the classes of the largest replicas first: their CTAs take SMs first
+    for (int c = clmd_ensemble::kClasses - 1; c >= 0; c--) {
       if (L[c].nitems == 0) continue;
       ECK(cudaStreamWaitEvent(E->cstream[c], E->evj, 0));
       int st = enqueue_class(E, c, L[c], nwin, balanced, capturing);
@@ -1721,8 +2156,9 @@ static int autotune(clmd_ensemble* E) {
   }
   for (int k = 0; k < kCand; k++) {
     int th[clmd_ensemble::kClasses];
-    for (int c = 0; c < clmd_ensemble::kClasses; c++) th[c] = cand[k];
-    for (int c = 0; c < clmd_ensemble::kClasses; c++) {
+    for (int c = 0; c < clmd_ensemble::kClasses; c++)
+      th[c] = c < clmd_ensemble::kCtaClasses ? cand[k] : E->cls_threads[c];
+    for (int c = 0; c < clmd_ensemble::kCtaClasses; c++) {
       int st = launch_all(E, 1, th, 0.0f, c);
       if (st) return st;
       if (E->last_ms[c] < 0 || E->last_atoms[c] == 0) continue;
@@ -1733,7 +2169,28 @@ static int autotune(clmd_ensemble* E) {
       }
     }
   }
-  for (int c = 0; c < clmd_ensemble::kClasses; c++) E->cls_threads[c] = pick[c];
+  // second axis (mixed precision): lanes per atom in the force pass, with
+  // each class's shape from the first stage
+  if (E->cfg.precision == CLMD_PREC_MIXED) {
+    for (int lg = 1; lg <= 2; lg++) {
+      int th[clmd_ensemble::kClasses];
+      for (int c = 0; c < clmd_ensemble::kClasses; c++)
+        th[c] = c < clmd_ensemble::kCtaClasses ? (pick[c] & ~(0xff << CLMD_ENS_LANES_SHIFT)) |
+                                                     (lg << CLMD_ENS_LANES_SHIFT)
+                                               : E->cls_threads[c];
+      for (int c = 0; c < clmd_ensemble::kCtaClasses; c++) {
+        int st = launch_all(E, 1, th, 0.0f, c);
+        if (st) return st;
+        if (E->last_ms[c] < 0 || E->last_atoms[c] == 0) continue;
+        float per_atom = E->last_ms[c] / (float)E->last_atoms[c];
+        if (per_atom < best[c]) {
+          best[c] = per_atom;
+          pick[c] = th[c];
+        }
+      }
+    }
+  }
+  for (int c = 0; c < clmd_ensemble::kCtaClasses; c++) E->cls_threads[c] = pick[c];
   E->tuned = true;
   return CLMD_OK;
 }
@@ -1755,7 +2212,7 @@ extern "C" int clmd_ens_autotune(clmd_ensemble* E, int32_t* threads_out) {
   std::lock_guard<std::mutex> lock(E->mu);
   int st = autotune(E);
   if (threads_out)
-    for (int c = 0; c < clmd_ensemble::kClasses; c++) threads_out[c] = E->cls_threads[c];
+    for (int c = 0; c < clmd_ensemble::kCtaClasses; c++) threads_out[c] = E->cls_threads[c];
   return st;
 }
 
@@ -2049,9 +2506,18 @@ extern "C" int clmd_ens_download(clmd_ensemble* E, double* x, double* y, double*
 
 extern "C" int clmd_ens_last_ms(clmd_ensemble* E, float* ms, int64_t* atoms) {
   if (!E) return CLMD_ERR_ARG;
-  for (int c = 0; c < clmd_ensemble::kClasses; c++) {
-    if (ms) ms[c] = E->last_ms[c];
-    if (atoms) atoms[c] = E->last_atoms[c];
+  // four entries: the single-CTA classes 0-2, then class 3 together with the
+  // cluster classes (the longest of their times, the sum of their atoms)
+  for (int c = 0; c < clmd_ensemble::kCtaClasses; c++) {
+    float m = E->last_ms[c];
+    long long a = E->last_atoms[c];
+    if (c == clmd_ensemble::kCtaClasses - 1)
+      for (int k = clmd_ensemble::kCtaClasses; k < clmd_ensemble::kClasses; k++) {
+        m = std::max(m, E->last_ms[k]);
+        a += E->last_atoms[k];
+      }
+    if (ms) ms[c] = m;
+    if (atoms) atoms[c] = a;
   }
   return CLMD_OK;
 }

@@ -274,9 +274,14 @@ int clmd_ens_add(clmd_ensemble* e, const clmd_replica_spec* spec, const double* 
                  const double* vz, int32_t* slot);
 /* Advances every running replica by up to nwin windows of ftcsi steps (one
  * persistent launch per size class, the classes concurrently); replicas stop
- * when done.  The launch sequence is captured once into a CUDA graph and
- * replayed while the set of running replicas and the launch shapes stay the
- * same (CLMD_ENS_GRAPHS=0 in the environment at creation: direct launches). */
+ * when done.  A replica runs on one CTA, or -- when its positions do not fit
+ * in one SM's shared memory (about 9,000 atoms and more) -- on a
+ * thread-block cluster of 2, 4, 8 or 16 CTAs (about 3,072 atoms per CTA or
+ * more) that splits its atoms and meets at cluster barriers
+ * (CLMD_ENS_CLUSTERS=0 in the environment at creation: one CTA each).  The
+ * launch sequence is captured once into a CUDA graph and replayed while the
+ * set of running replicas and the launch shapes stay the same
+ * (CLMD_ENS_GRAPHS=0 in the environment at creation: direct launches). */
 int clmd_ens_step(clmd_ensemble* e, int32_t nwin);
 /* Balanced step for mixed sizes: every running replica advances for about
  * ms of device time (at least one MD step), from the time per step the
@@ -291,11 +296,16 @@ int clmd_ens_step_timed(clmd_ensemble* e, float ms);
  * memory allows; the plain shapes allow up to 128 registers below 1024
  * threads). */
 #define CLMD_ENS_LEAN 0x10000
+/* Block shape field: lanes per atom in the mixed-precision force pass,
+ * 1 << ((shape >> CLMD_ENS_LANES_SHIFT) & 3), i.e. 1, 2 or 4 (consecutive
+ * lanes share an atom's row and merge their Kahan sums in a fixed tree). */
+#define CLMD_ENS_LANES_SHIFT 20
 /* Autotuner: picks the block shape of each of the 4 replica-size classes
  * (atoms <= 2048, <= 4096, <= 6144, larger) from 128, 256, 512, 1024 and
  * the CLMD_ENS_LEAN 128, 256 and 512 by timing one window per candidate and
- * class, each class alone on the GPU, on the running replicas; every replica
- * advances by those 7 windows.  threads_out (4 entries, may be NULL) gets the choice (threads
+ * class, each class alone on the GPU, on the running replicas; then, in
+ * mixed precision, the lanes per atom of the force pass (1, 2 or 4) with
+ * that shape.  Every replica advances by those 7 (+ 2) windows.  threads_out (4 entries, may be NULL) gets the choice (threads
  * in the low 16 bits).  Without it the classes use lean 512, 1024, 1024 and
  * 1024 threads (the tuner's picks on the batched workload), or
  * clmd_ens_config.threads for all if that is set (the flag allowed). */
@@ -383,7 +393,9 @@ int clmd_thermostat_clu(clmd_system* sys, int32_t step, char eclth, int32_t eclt
  * sqrt((<t^2> - <t>^2) / count).  Steps, not time: multiply by dt. */
 int clmd_ens_mfpt(clmd_ensemble* e, int32_t cap, double* mean, double* sem, int32_t* count);
 /* Device time (ms, CUDA events) of the last window's launch of each of the 4
- * size classes (-1 if the class was empty) and the atoms it advanced. */
+ * size classes (-1 if the class was empty) and the atoms it advanced; the
+ * fourth entry also covers the replicas run on thread-block clusters (the
+ * longest of those launches, the sum of their atoms). */
 int clmd_ens_last_ms(clmd_ensemble* e, float* ms, int64_t* atoms);
 /* Atoms currently free in the pool. */
 int64_t clmd_ens_free_atoms(clmd_ensemble* e);

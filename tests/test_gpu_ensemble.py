@@ -47,7 +47,9 @@ def force_errors(st, ref):
 @pytest.mark.parametrize("precision,tol,threads", [
     (clmd.PREC_MIXED, 1e-5, 0), (clmd.PREC_FP64, 1e-12, 0),
     (clmd.PREC_MIXED, 1e-5, 256 | clmd.ENS_LEAN), (clmd.PREC_MIXED, 1e-5, 512 | clmd.ENS_LEAN),
-    (clmd.PREC_FP64, 1e-12, 128 | clmd.ENS_LEAN)])
+    (clmd.PREC_FP64, 1e-12, 128 | clmd.ENS_LEAN),
+    (clmd.PREC_MIXED, 1e-5, 1024 | clmd.ens_lanes(2)),
+    (clmd.PREC_MIXED, 1e-5, 256 | clmd.ENS_LEAN | clmd.ens_lanes(4))])
 def test_ensemble_forces_against_oracle(gpu, precision, tol, threads):
     """Every block shape the autotuner may pick (the default per-class
     shapes and the register-lean ones) against the FP64 oracle."""
@@ -505,3 +507,82 @@ def test_failed_replica_is_isolated(gpu):
         xa, _ = a.state(p)
         xb, _ = b.state(q)
         assert np.array_equal(xa.x, xb.x) and np.array_equal(xa.vz, xb.vz)
+
+
+CLUSTER_SIZES = [(12000, 0.03), (26000, 0.02), (52000, 0.04)]  # 4, 16 and 16 CTAs
+
+
+@pytest.mark.parametrize("precision,tol", [(clmd.PREC_MIXED, 1e-5), (clmd.PREC_FP64, 1e-12)])
+def test_cluster_replicas_against_oracle(gpu, precision, tol):
+    """Replicas too large for one SM's shared memory run on thread-block
+    clusters (2-16 CTAs, positions in global memory, cluster barriers and
+    distributed-shared-memory reductions).  After two windows with list
+    rebuilds and analyses: forces on the engine's positions against the FP64
+    oracle (1e-5 mixed, 1e-12 FP64) and the Stillinger labels bit-exact."""
+    e = clmd.Ensemble(clmd.ens_config(sum(n for n, _ in CLUSTER_SIZES) + 1000, 4,
+                                      precision=precision, ftcsi=25))
+    slots = []
+    for k, (n, rho) in enumerate(CLUSTER_SIZES):
+        box, arrs = replica_inputs(n, rho, 0.7, 300 + k)
+        slots.append((e.add(n, box, 0.7, *arrs, csover=10**6), n, box))
+    e.step(2)
+    res = e.results()
+    states = {}
+    for s, n, box in slots:
+        r = res[s]
+        assert r.status == 0 and r.step == 50 and r.nrebuild >= 3, (n, r.status, r.step)
+        st, _ = e.state(s)  # positions at the next analysis step
+        states[s] = st
+        norm, per_atom = force_errors(st, oracle_forces(n, box, st).get_state())
+        assert norm <= tol and per_atom <= 10 * tol, (n, norm, per_atom)
+    e.step(1)  # opens with the analysis of those positions
+    for s, n, box in slots:
+        st = states[s]
+        _, cl = e.state(s)
+        cfg = clmd.lj_config(n, n / box ** 3, 0.7)
+        o = orc.Oracle(cfg, neighbor_mode=1, label_mode=1)
+        z0 = np.zeros(n)
+        o.set_state(clmd.State(st.x, st.y, st.z, z0, z0, z0, z0, z0, z0),
+                    scalars=orc.scalars_init(cfg))
+        o.neighbor(0)
+        o.stoddard(0)
+        assert np.array_equal(cl, o.clusters()["cl"]), n
+        assert e.results()[s].step == 75
+
+
+def test_cluster_replica_matches_single_cta_and_mix(gpu, monkeypatch):
+    """The same large replica on a cluster, alone and beside small replicas
+    (bit-identical: its cluster size depends on its own size only), and on
+    one CTA (CLMD_ENS_CLUSTERS=0: the same steps, sums in another order,
+    so agreeing to rounding over one window)."""
+    n, rho, temp = 20000, 0.03, 0.7
+    box, arrs = replica_inputs(n, rho, temp, 77)
+
+    def run(extra, clusters=True):
+        if not clusters:
+            monkeypatch.setenv("CLMD_ENS_CLUSTERS", "0")
+        e = clmd.Ensemble(clmd.ens_config(n + 30000, 24, ftcsi=25))
+        monkeypatch.delenv("CLMD_ENS_CLUSTERS", raising=False)
+        rng = np.random.default_rng(4)
+        for k in range(extra):
+            m = int(rng.integers(300, 2500))
+            b2, a2 = replica_inputs(m, 0.04, 0.75, 2000 + k)
+            e.add(m, b2, 0.75, *a2, csover=51)
+        s = e.add(n, box, temp, *arrs, csover=10**6)
+        e.step(2)
+        st, cl = e.state(s)
+        r = e.results()[s]
+        e.close()
+        return st, cl, r
+
+    a, ca, ra = run(0)
+    b, cb, rb = run(12)
+    for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az"):
+        assert np.array_equal(getattr(a, k), getattr(b, k)), k
+    assert np.array_equal(ca, cb) and ra.psi == rb.psi and ra.step == rb.step == 50
+    c, cc, rc = run(0, clusters=False)
+    assert rc.step == 50 and rc.nrebuild == ra.nrebuild
+    for k in ("x", "y", "z"):
+        np.testing.assert_allclose(getattr(c, k), getattr(a, k), rtol=0, atol=1e-9 * box)
+    np.testing.assert_allclose(c.vx, a.vx, rtol=0, atol=1e-8)
+    assert abs(rc.psi - ra.psi) <= 1e-9 * abs(ra.psi) + 1e-14
