@@ -894,6 +894,7 @@ def batched_arm(args):
     l0 = e.launches()
     clocks = Clocks(dev)
     kern_ms, kern_bytes = [], []
+    pt0 = e.pair_terms()
     barrier()
     clocks.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -915,6 +916,7 @@ def batched_arm(args):
     units = rk.sum(float(atom_steps))
     value = units / el_max
     launches = e.launches() - l0
+    pair_terms = e.pair_terms() - pt0
 
     # ---- roofline: the window kernels (size classes run concurrently)
     peak, peak_kind = measured_peaks()
@@ -985,7 +987,17 @@ def batched_arm(args):
                                    "4 size classes concurrently)",
                          "algorithmic_bytes_per_atom_step": BYTES_PER_ATOM_STEP_MIXED,
                          "kernel_ms_per_window": statistics.mean(kern_ms),
-                         "peak_kind": peak_kind},
+                         "peak_kind": peak_kind,
+                         "limiter": {
+                             "what": "issue- and latency-bound, not HBM: each replica's working "
+                                     "set stays in shared memory and L2 (DRAM traffic is a "
+                                     "tenth of the algorithmic bytes); the work is the pair "
+                                     "terms (FP64 minimum image + cut-off test, FP32 LJ "
+                                     "term) and the per-step phases between barriers",
+                             "pair_terms_per_s": pair_terms / (sum(kern_ms) / 1e3),
+                             "pair_terms_per_atom_step": pair_terms / max(1.0, atom_steps),
+                             "ncu": "profiles/k_ens_batched.md (lanes per warp instruction, "
+                                    "warps active, issue active, FP64/FP32 pipes)"}},
             "cpu_baseline": cpu,
             "clocks": clk,
             "fp64_ensemble_same_ensemble": fp64_value,

@@ -307,6 +307,7 @@ def load(path: str = LIB_PATH):
         "clmd_ens_download": ([P, d, d, d, d, d, d], C.c_int),
         "clmd_ens_free_atoms": ([P], C.c_int64),
         "clmd_ens_launches": ([P], C.c_int64),
+        "clmd_ens_pair_terms": ([P, C.POINTER(C.c_int64)], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -760,3 +761,11 @@ class Ensemble:
 
     def launches(self):
         return self.lib.clmd_ens_launches(self.h)
+
+    def pair_terms(self):
+        """Pair terms the force passes of the current replicas evaluated."""
+        t = C.c_int64(0)
+        st = self.lib.clmd_ens_pair_terms(self.h, C.byref(t))
+        if st:
+            raise ClmdError(st, "clmd_ens_pair_terms")
+        return t.value

@@ -57,6 +57,8 @@ struct Rep {
   // slot to its atom): 1 (positions too large for shared memory) cell order,
   // 2 (the others) by the rows' lengths; both renewed at every rebuild
   int reorder;
+  int nfull;                // full-list entries (pair terms per force pass) of the last rebuild
+  long long pterms;         // pair terms evaluated by this replica's force passes
 };
 
 struct Args {
@@ -629,7 +631,7 @@ __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
   }
   const double hL = 0.5 * L, rs2 = C.rs2;
   const long long lbase = (long long)off * A.lstride;
-  int over = 0;
+  int over = 0, nsum = 0;
   for (int i = gt; i < N; i += GT) {
     const double xi = P.x(i), yi = P.y(i), zi = P.z(i);
     int cx = min((int)(xi * C.cf), C.ncx - 1), cy = min((int)(yi * C.cf), C.ncx - 1),
@@ -693,8 +695,15 @@ __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
       n = A.lstride;
     }
     A.rlen[off + i] = n;
+    nsum += n;
   }
-  over = grp_or<NT, CS>(over, C);
+  {
+    // the rows' total (pair terms of each force pass until the next
+    // rebuild) and "any row overflowed" in one reduction
+    double tn = (double)nsum, unused = 0.0;
+    grp_sum2<NT, CS>(tn, unused, over, C);
+    if (tid == 0) R.nfull = (int)tn;
+  }
   if (over) {
     if (tid == 0 && R.status == 0) R.status = CLMD_ERR_LIST_OVERFLOW;
     gsync<CS>();
@@ -1291,7 +1300,10 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
           }
         }
       }
-      if (tid == 0) R.step = step + 1;
+      if (tid == 0) {
+        R.step = step + 1;
+        R.pterms += R.nfull;
+      }
       gsync<CS>();
     }
     // a spent budget ends the replica at once, after the analysis due at its
@@ -1786,6 +1798,18 @@ extern "C" int64_t clmd_ens_free_atoms(clmd_ensemble* E) {
 }
 
 extern "C" int64_t clmd_ens_launches(clmd_ensemble* E) { return E ? E->launches : 0; }
+
+extern "C" int clmd_ens_pair_terms(clmd_ensemble* E, int64_t* total) {
+  if (!E || !total) return CLMD_ERR_ARG;
+  std::lock_guard<std::mutex> lock(E->mu);
+  int rs = refresh_reps(E);
+  if (rs) return rs;
+  long long t = 0;
+  for (int s = 0; s < E->cfg.max_replicas; s++)
+    if (E->used[s]) t += E->h_reps[s].pterms;
+  *total = t;
+  return CLMD_OK;
+}
 
 extern "C" int clmd_ens_add(clmd_ensemble* E, const clmd_replica_spec* sp, const double* x,
                             const double* y, const double* z, const double* vx,

@@ -397,6 +397,11 @@ int clmd_ens_mfpt(clmd_ensemble* e, int32_t cap, double* mean, double* sem, int3
  * fourth entry also covers the replicas run on thread-block clusters (the
  * longest of those launches, the sum of their atoms). */
 int clmd_ens_last_ms(clmd_ensemble* e, float* ms, int64_t* atoms);
+/* Pair terms (full neighbour-list entries, each an FP64 minimum image and
+ * cut-off test and, within rc, an LJ term) the force passes of all current
+ * replicas have evaluated since admission: the work measure of the force
+ * kernel. */
+int clmd_ens_pair_terms(clmd_ensemble* e, int64_t* total);
 /* Atoms currently free in the pool. */
 int64_t clmd_ens_free_atoms(clmd_ensemble* e);
 /* Kernel launches issued so far. */

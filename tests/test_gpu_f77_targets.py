@@ -100,6 +100,13 @@ def test_nose_target_integrator_per_call(gpu, monkeypatch):
     o = orc.Oracle(cfg)
     o.set_state(clmd.State(*arrs, z0, z0, z0), scalars=orc.scalars_init(cfg))
     o.stopdead(-1)
+    # the same list and accelerations on both sides: neighbor(0) + AccAtom
+    # on the post-stopdead state (main.f's start)
+    put_state(lib, n, o.get_state())
+    put_scalars(lib, o.scalars())
+    s = C.c_int32(0)
+    lib.neighbor_(C.byref(s))
+    lib.accatom_()
     o.neighbor(0)
     o.zero_acc()
     o.accatom()
