@@ -943,16 +943,17 @@ def batched_arm(args):
     d2h = 6 * 8 * total + 16 * len(slots)
 
     line = None
-    extra = {}
-    if rank == 0:
+    extra = dict(pcheck=None, rates=[], dropin_value=None)
+    ferr_n = ferr_a = None
+    if rank == 0 and not args.no_extras:
         ferr_n, ferr_a = mixed_force_error(e, slots, slots)
     e.close()
     rk.barrier()
     # ---- the same replicas as an all-FP64 ensemble (same kernels, FP64
     # pair terms and sums): how much of the gain is batching, how much
     # mixed precision
-    fp64_value, fp64_tuned = fp64_ensemble_rate(specs, args)
-    if rank == 0:
+    fp64_value, fp64_tuned = (None, []) if args.no_extras else fp64_ensemble_rate(specs, args)
+    if rank == 0 and not args.no_extras:
         pcheck = precision_check(specs)
         order = sorted(slots, key=lambda k: slots[k][0])
         picks = [order[int(q * (len(order) - 1))] for q in np.linspace(0, 1, args.dropin_sample)]
@@ -964,7 +965,7 @@ def batched_arm(args):
         dropin_value = sum(slots[k][0] * 100 for k in slots) / t_drop
         extra = dict(pcheck=pcheck, rates=rates, dropin_value=dropin_value)
     # ---- served leg: a bounded Poisson window on this GPU
-    served = None if args.no_served else served_leg(args, rk)
+    served = None if (args.no_served or args.no_extras) else served_leg(args, rk)
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
@@ -1002,9 +1003,9 @@ def batched_arm(args):
             "clocks": clk,
             "fp64_ensemble_same_ensemble": fp64_value,
             "fp64_ensemble_threads_per_size_class": [clmd.shape_name(t) for t in fp64_tuned],
-            "speedup_vs_fp64_ensemble": value / fp64_value,
+            "speedup_vs_fp64_ensemble": value / fp64_value if fp64_value else None,
             "fp64_dropin_same_ensemble": dropin_value,
-            "speedup_vs_fp64_dropin": value / dropin_value,
+            "speedup_vs_fp64_dropin": value / dropin_value if dropin_value else None,
             "dropin_sample_rates": [[n, r] for n, r in extra["rates"]],
             "force_rel_err_vs_fp64": {"normwise": ferr_n, "worst_atom": ferr_a},
             "mixed_vs_fp64_sample": extra["pcheck"],
@@ -1144,6 +1145,38 @@ def served_summary(out, st, nreq, serve_s):
     }
 
 
+def big_replica_ms_per_step(n=50000, rho=0.03, temp=0.75, windows=3):
+    """Device ms per MD step of one n-atom replica alone on the GPU (the
+    served workload's largest size), on a thread-block cluster and, with
+    CLMD_ENS_CLUSTERS=0, on one CTA: (cluster ms, single-CTA ms, CTAs)."""
+    import torch
+    out = []
+    for clusters in (True, False):
+        if not clusters:
+            os.environ["CLMD_ENS_CLUSTERS"] = "0"
+        try:
+            e = clmd.Ensemble(clmd.ens_config(n + 16, 2, precision=clmd.PREC_MIXED,
+                                              integrator=clmd.INT_NOSE, ftcsi=100))
+        finally:
+            os.environ.pop("CLMD_ENS_CLUSTERS", None)
+        box = (n / rho) ** (1.0 / 3.0)
+        x, y, z, vx, vy, vz = clmd.init_random(n, (box, box, box), 0.9, temp, 4242)
+        slot = e.add(n, box, temp, x, y, z, vx, vy, vz, csover=10**6, budget=0)
+        e.step(1)
+        torch.cuda.synchronize()
+        s0 = e.results()[slot].step
+        t = time.perf_counter()
+        e.step(windows)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t
+        out.append(el * 1e3 / (e.results()[slot].step - s0))
+        e.close()
+    cs = 2
+    while cs < 16 and cs * 3072 < n:
+        cs *= 2
+    return out[0], out[1], cs
+
+
 def served_leg(args, rk):
     """configs[4] inside the default bench: a bounded Poisson window at 200
     requests/s (N log-uniform in [100, 50000], rho* and T* uniform, budgets
@@ -1160,6 +1193,12 @@ def served_leg(args, rk):
          "value": units / wall, "unit": "atom-steps/s", "gpu_launches": int(launches),
          "pool_atoms": pool, "max_resident_replicas": args.served_slots, "clocks": clk}
     d.update(served_summary(out, st, len(reqs), args.served_cap))
+    if rk.rank == 0:
+        cl_ms, cta_ms, cs = big_replica_ms_per_step()
+        d["one_replica_50000_atoms"] = {
+            "ms_per_step_cluster": cl_ms, "ms_per_step_one_cta": cta_ms,
+            "cluster_ctas": cs, "speedup": cta_ms / cl_ms,
+            "note": "alone on the GPU, whole 100-step windows, host clock"}
     return d
 
 
@@ -1245,6 +1284,9 @@ def main():
     ap.add_argument("--dropin-sample", type=int, default=8)
     ap.add_argument("--no-served", action="store_true",
                     help="batched: leave out the served leg")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="batched: only value, e2e and roofline (no FP64 comparisons, "
+                         "precision check or served leg; for profiler runs)")
     ap.add_argument("--served-arrival", type=float, default=10.0,
                     help="batched: Poisson arrival window of the served leg (s)")
     ap.add_argument("--served-cap", type=float, default=30.0,

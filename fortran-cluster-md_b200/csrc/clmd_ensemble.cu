@@ -181,6 +181,45 @@ __device__ __forceinline__ bool cta_nh_root(double S, double psi1, double nkt3, 
   return sh[34] != 0.0;
 }
 
+// cta_nh_root with the step's end folded in (one CTA per replica): lane 0
+// of warp 0 also records the replica's new PSI, sum v^2, ekin, step and pair
+// terms (or the solve's failure) before the barrier that publishes the root,
+// so the step needs no barrier of its own to publish them
+template <int NT>
+__device__ __forceinline__ bool cta_nh_root_commit(double S, double psi1, double nkt3,
+                                                   double dth, double Q, double* sh, Rep& R,
+                                                   int step, double& p) {
+  constexpr int W = NT / 32;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  S = wsum(S);
+  if (lane == 0) sh[w] = S;
+  __syncthreads();
+  if (w == 0) {
+    const double t = wsum(lane < W ? sh[lane] : 0.0);
+    double pr;
+    const bool ok = clmd_nh_root(t, psi1, nkt3, dth, Q, pr);
+    if (lane == 0) {
+      // slots 100, 101: past every slot a reduction of the next step writes
+      // (up to 3 * 32), since no barrier separates these reads from them
+      sh[100] = pr;
+      sh[101] = ok ? 1.0 : 0.0;
+      if (ok) {
+        const double vsc = 1.0 / (1.0 + dth * pr);
+        R.sumv2 = t * vsc * vsc;
+        R.psi = pr;
+        R.ekin = 0.5 * R.sumv2;
+        R.step = step + 1;
+        R.pterms += R.nfull;
+      } else if (R.status == 0) {
+        R.status = CLMD_ERR_NH_NOCONVERGE;
+      }
+    }
+  }
+  __syncthreads();
+  p = sh[100];
+  return sh[101] != 0.0;
+}
+
 // block max of a and sum of b in one round (as cta_sum2)
 template <int NT>
 __device__ __forceinline__ void cta_maxsum(double& a, double& b, double* sh) {
@@ -632,34 +671,52 @@ __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
   const double hL = 0.5 * L, rs2 = C.rs2;
   const long long lbase = (long long)off * A.lstride;
   int over = 0, nsum = 0;
-  for (int i = gt; i < N; i += GT) {
+  // the atoms in cell order (sorted[]), whatever order their slots have: the
+  // lanes of a warp then search overlapping stencils (similar candidate
+  // counts, the same candidates read by several lanes at once)
+  for (int q0 = gt; q0 < N; q0 += GT) {
+    const int i = A.sorted[off + q0];
     const double xi = P.x(i), yi = P.y(i), zi = P.z(i);
     int cx = min((int)(xi * C.cf), C.ncx - 1), cy = min((int)(yi * C.cf), C.ncx - 1),
         cz = min((int)(zi * C.cf), C.ncx - 1);
     int n = 0;
+    // with three or more cells per dimension the stencil's cells hold each
+    // neighbour once, at the periodic image nearest to atom i for every pair
+    // within the list radius (cells are at least that wide): the image
+    // shift is the cell range's, added to xi - xj with the same single
+    // rounding the minimum image (mi_sel) gives, so the pair set and r^2
+    // are those of mi_sel without its per-candidate tests; r^2 does not
+    // depend on the pair's orientation (IEEE subtraction is sign-symmetric)
+    const bool sel = C.nox < 3;
     for (int a = 0; a < C.nox; a++) {
       int zz = cz + C.offx[a];
+      const double szL = sel ? 0.0 : (zz < 0 ? L : (zz >= C.ncx ? -L : 0.0));
       zz += zz < 0 ? C.ncx : 0;
       zz -= zz >= C.ncx ? C.ncx : 0;
       for (int b = 0; b < C.nox; b++) {
         int yy = cy + C.offx[b];
+        const double syL = sel ? 0.0 : (yy < 0 ? L : (yy >= C.ncx ? -L : 0.0));
         yy += yy < 0 ? C.ncx : 0;
         yy -= yy >= C.ncx ? C.ncx : 0;
         // the x-neighbours of a cell row are contiguous in cell order: one
         // candidate range, two where the row wraps (all of it when ncx <= 2)
         const int rowc = (zz * C.ncx + yy) * C.ncx;
         int ra[2], rb[2], nr = 1;
-        if (C.nox < 3) {
+        double sxr[2] = {0.0, 0.0};
+        if (sel) {
           ra[0] = rowc; rb[0] = rowc + C.ncx;
         } else if (cx == 0) {
           ra[0] = rowc; rb[0] = rowc + 2; ra[1] = rowc + C.ncx - 1; rb[1] = rowc + C.ncx; nr = 2;
+          sxr[1] = L;
         } else if (cx == C.ncx - 1) {
           ra[0] = rowc + cx - 1; rb[0] = rowc + C.ncx; ra[1] = rowc; rb[1] = rowc + 1; nr = 2;
+          sxr[1] = -L;
         } else {
           ra[0] = rowc + cx - 1; rb[0] = rowc + cx + 2;
         }
         for (int d = 0; d < nr; d++) {
           const int q1 = C.cstart[rb[d]];
+          const double sxL = sxr[d];
           // four candidates' indices loaded ahead of their tests
           for (int q = C.cstart[ra[d]]; q < q1; q += 4) {
             int js[4];
@@ -669,16 +726,17 @@ __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
             for (int u = 0; u < 4; u++) {
               const int j = js[u];
               if (j == i) continue;
-              // the pair in the reference's orientation (row of the smaller index)
-              double dx, dy, dz;
-              if (i < j) {
-                dx = xi - P.x(j); dy = yi - P.y(j); dz = zi - P.z(j);
+              double dx = __dsub_rn(xi, P.x(j)), dy = __dsub_rn(yi, P.y(j)),
+                     dz = __dsub_rn(zi, P.z(j));
+              if (sel) {
+                dx = mi_sel(dx, L, hL);
+                dy = mi_sel(dy, L, hL);
+                dz = mi_sel(dz, L, hL);
               } else {
-                dx = P.x(j) - xi; dy = P.y(j) - yi; dz = P.z(j) - zi;
+                dx = __dadd_rn(dx, sxL);
+                dy = __dadd_rn(dy, syL);
+                dz = __dadd_rn(dz, szL);
               }
-              dx = mi_sel(dx, L, hL);
-              dy = mi_sel(dy, L, hL);
-              dz = mi_sel(dz, L, hL);
               double r2 =
                   __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
               if (r2 <= rs2) {
@@ -925,7 +983,10 @@ __device__ void forces(Rep& R, Cta& C, const Args& A, const Pos<SM>& P, bool kic
       if (kick) R.ekin = k;
     }
   }
-  gsync<CS>();
+  // one CTA, mixed Nose-Hoover: the closed-form root that follows opens with
+  // barriers of its own (cta_nh_root_commit), which order this pass's
+  // per-atom writes before anyone reads them
+  if constexpr (!(NHF && MIXED && CS == 1)) gsync<CS>();
 }
 
 template <bool MIXED>
@@ -1158,6 +1219,7 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
     {
       // energies at the end of every window and of the launch
       const bool last = todo == 1 || (R.step + 1) % (A.ftcsi > 0 ? A.ftcsi : 1) == 0;
+      bool committed = false;  // the step's end already recorded (uniform)
       const int step = R.step;
       // drift
       double d2 = 0.0, sv = 0.0;
@@ -1200,8 +1262,30 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
         A.vz[off + i] = vzi;
         d2 = fmax(d2, dx * dx + dy * dy + dz * dz);
       }
-      grp_maxsum<NT, CS>(d2, sv, C);
-      const double dmmr = d2, sumv2 = sv;
+      // the step's scalar logic on thread 0 (the reference's NH half step of
+      // PSI and s, int-verlet-mav.f:64-74 skin bookkeeping, the rebuild
+      // decision); one CTA: warp 0 takes the block totals between the two
+      // barriers (the same tree as cta_maxsum), so one barrier fewer
+      double dmmr = 0.0, sumv2 = 0.0;
+      if constexpr (CS == 1) {
+        constexpr int W = NT / 32;
+        const int lane = tid & 31, w = tid >> 5;
+        d2 = wmax(d2);
+        sv = wsum(sv);
+        if (lane == 0) {
+          C.red[w] = d2;
+          C.red[W + w] = sv;
+        }
+        __syncthreads();
+        if (w == 0) {
+          dmmr = wmax(lane < W ? C.red[lane] : 0.0);
+          sumv2 = wsum(lane < W ? C.red[W + lane] : 0.0);
+        }
+      } else {
+        grp_maxsum<NT, CS>(d2, sv, C);
+        dmmr = d2;
+        sumv2 = sv;
+      }
       if (tid == 0) {
         if (nh) {
           R.sumv2 = sumv2;
@@ -1227,18 +1311,24 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
         if (MIXED) {
           double S = 0.0, unused = 0.0, p;
           forces<NT, SM, MIXED, CS, true>(R, C, A, P, false, last, psi1, dtQ, &S, &unused);
-          if (!grp_nh_root<NT, CS>(S, psi1, R.nkt3_i, dth, Q, C, S, p)) {
-            if (tid == 0 && R.status == 0) R.status = CLMD_ERR_NH_NOCONVERGE;
-            gsync<CS>();
-            goto out;
+          if constexpr (CS == 1) {
+            if (!cta_nh_root_commit<NT>(S, psi1, R.nkt3_i, dth, Q, C.red, R, step, p)) goto out;
+            committed = true;
+          } else {
+            if (!grp_nh_root<NT, CS>(S, psi1, R.nkt3_i, dth, Q, C, S, p)) {
+              if (tid == 0 && R.status == 0) R.status = CLMD_ERR_NH_NOCONVERGE;
+              gsync<CS>();
+              goto out;
+            }
+            if (tid == 0) {
+              const double c = 1.0 / (1.0 + dth * p);
+              R.sumv2 = S * c * c;
+              R.psi = p;
+              R.ekin = 0.5 * R.sumv2;
+            }
           }
           vsc = 1.0 / (1.0 + dth * p);
           vin_n = true;
-          if (tid == 0) {
-            R.sumv2 = S * vsc * vsc;
-            R.psi = p;
-            R.ekin = 0.5 * R.sumv2;
-          }
         } else {
           double sumv2n = 0.0, dpsum = 0.0;
           forces<NT, SM, MIXED, CS, true>(R, C, A, P, false, last, psi1, dtQ, &sumv2n, &dpsum);
@@ -1300,11 +1390,13 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
           }
         }
       }
-      if (tid == 0) {
-        R.step = step + 1;
-        R.pterms += R.nfull;
+      if (!committed) {
+        if (tid == 0) {
+          R.step = step + 1;
+          R.pterms += R.nfull;
+        }
+        gsync<CS>();
       }
-      gsync<CS>();
     }
     // a spent budget ends the replica at once, after the analysis due at its
     // last step, rather than at the start of the next launch
@@ -2066,9 +2158,24 @@ static int launch_all(clmd_ensemble* E, int nwin, const int* threads, float min_
   const bool balanced = min_ms > 0.0f;
   if (balanced && total > 0) {
     const int win = E->cfg.ftcsi > 0 ? E->cfg.ftcsi : 1;
+    // while every replica's CTAs fit on the GPU at once, each runs for about
+    // min_ms; when they do not (they then take turns on the SMs), each gets
+    // about min_ms of SM time: a replica on a cluster of cs CTAs runs 1 / cs
+    // of the steps that would fill min_ms, so that large replicas do not
+    // take the SMs from the small ones in proportion to their cluster size
+    long long demand = 0;
+    int k0 = 0;
+    std::vector<int> item_cs(total, 1);
+    for (int c = 0; c < clmd_ensemble::kClasses; c++) {
+      for (size_t q = 0; q < cls[c].size(); q++) item_cs[k0 + q] = E->cls_cs[c];
+      demand += (long long)cls[c].size() * E->cls_cs[c];
+      k0 += (int)cls[c].size();
+    }
+    const bool shared = demand > E->nsm;
     for (int k = 0; k < total; k++) {  // a replica not timed yet runs a few steps
       const float t = E->h_wtime[E->h_items[k]];  // ms per step, 0 = not timed yet
-      long long n = t > 0.0f ? (long long)(min_ms / t) : (long long)std::min(win, 10);
+      const float ms = shared ? min_ms / (float)item_cs[k] : min_ms;
+      long long n = t > 0.0f ? (long long)(ms / t) : (long long)std::min(win, 10);
       E->h_iwin[k] = (int)std::max(1LL, std::min(n, (long long)1 << 24));
     }
     ECK(cudaMemcpyAsync(E->d_iwin, E->h_iwin, sizeof(int) * total, cudaMemcpyHostToDevice,

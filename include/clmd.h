@@ -286,7 +286,9 @@ int clmd_ens_step(clmd_ensemble* e, int32_t nwin);
 /* Balanced step for mixed sizes: every running replica advances for about
  * ms of device time (at least one MD step), from the time per step the
  * kernel measured for it in earlier launches (a replica not yet timed runs
- * a few steps).  Small replicas then do not idle while the largest finish,
+ * a few steps); when the replicas' CTAs cannot all be resident at once, a
+ * replica on a cluster of c CTAs runs for about ms / c instead (the same SM
+ * time as a single-CTA replica).  Small replicas then do not idle while the largest finish,
  * and a launch lasts about ms whatever the sizes.  Launch boundaries may
  * fall inside a window: the analysis still runs at every multiple of ftcsi,
  * and trajectories are those of clmd_ens_step. */
