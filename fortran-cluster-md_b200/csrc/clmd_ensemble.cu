@@ -40,6 +40,15 @@ namespace clmd_ens {
 namespace cg = cooperative_groups;
 
 constexpr int kFptCap = 128;  // first-passage sizes tracked per replica
+#ifndef CLMD_SEARCH_PRUNE
+#define CLMD_SEARCH_PRUNE 0
+#endif
+#ifndef CLMD_SEARCH_CHUNK
+#define CLMD_SEARCH_CHUNK 2
+#endif
+// list search: candidate indices loaded ahead of their tests (2: measured
+// best of 1, 2, 4 and 8 on the batched workload, all bit-identical)
+constexpr int kSearchChunk = CLMD_SEARCH_CHUNK;
 constexpr int kNcMax = 28;    // cells per dimension at most (cells never narrower than the list radius)
 
 struct Rep {
@@ -76,6 +85,7 @@ struct Args {
   double rc, atskin, dt;
   int nbtim, ftcsi, lstride, integrator, nwin;
   int lg;  // mixed force pass: 1 << lg lanes per atom (0: one thread per atom)
+  int reorder_every;  // length order renewed at every k-th rebuild (reorder 2)
   int ncmax;  // cells per dimension this launch's shared memory holds
   int4* summary;  // per slot: done, status, step, maxcs
   float* wtime;   // per slot: device ms per MD step in its last launch (one CTA)
@@ -284,6 +294,7 @@ struct Cta {
   int ncx, ncell, nox, offx[3];
   double cf, rs2;
   int flag;
+  int ident;  // sorted[] is the identity (the slots are in cell order)
   int rep;  // slot of the replica being run
   int nsteps;  // MD steps this replica runs in this launch
 };
@@ -586,6 +597,7 @@ __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
   int* cnt = C.cstart;
   if constexpr (CS > 1) cnt = A.cscr + (long long)(blockIdx.x / CS) * A.cscr_stride;
   for (int c = gt; c <= C.ncell; c += GT) cnt[c] = 0;
+  if (tid == 0) C.ident = 0;  // until a reorder into cell order below
   gsync<CS>();
   for (int i = gt; i < N; i += GT) {
     const double x = wrap_box(P.x(i), L), y = wrap_box(P.y(i), L), z = wrap_box(P.z(i), L);
@@ -619,7 +631,10 @@ __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
     A.sorted[off + c0 + r] = i;
   }
   gsync<CS>();
-  if ((!SM && R.reorder == 1) || R.reorder == 2) {
+  // the length order may be kept for a few rebuilds (rows change little
+  // between rebuilds); the search and the forces use whatever order the
+  // slots have, so skipping it changes nothing but the order
+  if (R.reorder == 1 || (R.reorder == 2 && R.nrebuild % A.reorder_every == 0)) {
     // reorder 1 (positions in global memory): the atoms move into cell
     // order, so that a warp's neighbour gathers fall within a few cells'
     // worth of memory.  reorder 2: a stable order by the previous rows'
@@ -666,6 +681,7 @@ __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
       else
         A.sorted[off + p] = p;  // the cells now hold consecutive slots
     }
+    if (tid == 0) C.ident = R.reorder == 1;
     gsync<CS>();
   }
   const double hL = 0.5 * L, rs2 = C.rs2;
@@ -674,8 +690,9 @@ __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
   // the atoms in cell order (sorted[]), whatever order their slots have: the
   // lanes of a warp then search overlapping stencils (similar candidate
   // counts, the same candidates read by several lanes at once)
+  const bool ident = C.ident;
   for (int q0 = gt; q0 < N; q0 += GT) {
-    const int i = A.sorted[off + q0];
+    const int i = ident ? q0 : A.sorted[off + q0];
     const double xi = P.x(i), yi = P.y(i), zi = P.z(i);
     int cx = min((int)(xi * C.cf), C.ncx - 1), cy = min((int)(yi * C.cf), C.ncx - 1),
         cz = min((int)(zi * C.cf), C.ncx - 1);
@@ -688,6 +705,18 @@ __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
     // are those of mi_sel without its per-candidate tests; r^2 does not
     // depend on the pair's orientation (IEEE subtraction is sign-symmetric)
     const bool sel = C.nox < 3;
+#if CLMD_SEARCH_PRUNE
+    // the atom's distances to its cell's faces: a neighbour row (and an end
+    // cell of a row) whose nearest point is farther than the list radius
+    // holds no neighbour and is skipped (a margin of 1e-9 L covers the
+    // rounding of the cell assignment).  Off by default: bit-identical, but
+    // 3% slower on the batched workload (the per-row tests cost more than
+    // the ~20% of candidates they save)
+    const double cw = 1.0 / C.cf, mg = 1e-9 * L;
+    const double fxl = fmax(xi - cx * cw - mg, 0.0), fxr = fmax((cx + 1) * cw - xi - mg, 0.0);
+    const double fyl = fmax(yi - cy * cw - mg, 0.0), fyr = fmax((cy + 1) * cw - yi - mg, 0.0);
+    const double fzl = fmax(zi - cz * cw - mg, 0.0), fzr = fmax((cz + 1) * cw - zi - mg, 0.0);
+#endif
     for (int a = 0; a < C.nox; a++) {
       int zz = cz + C.offx[a];
       const double szL = sel ? 0.0 : (zz < 0 ? L : (zz >= C.ncx ? -L : 0.0));
@@ -703,27 +732,44 @@ __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
         const int rowc = (zz * C.ncx + yy) * C.ncx;
         int ra[2], rb[2], nr = 1;
         double sxr[2] = {0.0, 0.0};
+#if CLMD_SEARCH_PRUNE
+        bool lft = true, rgt = true;
+        if (!sel) {
+          const int oz = C.offx[a], oy = C.offx[b];
+          const double dz = oz < 0 ? fzl : (oz > 0 ? fzr : 0.0);
+          const double dy = oy < 0 ? fyl : (oy > 0 ? fyr : 0.0);
+          const double bx = rs2 - (dy * dy + dz * dz);
+          if (bx < 0.0) continue;
+          lft = fxl * fxl <= bx;
+          rgt = fxr * fxr <= bx;
+        }
+#else
+        const bool lft = true, rgt = true;
+#endif
         if (sel) {
           ra[0] = rowc; rb[0] = rowc + C.ncx;
         } else if (cx == 0) {
-          ra[0] = rowc; rb[0] = rowc + 2; ra[1] = rowc + C.ncx - 1; rb[1] = rowc + C.ncx; nr = 2;
+          ra[0] = rowc; rb[0] = rowc + (rgt ? 2 : 1);
+          ra[1] = rowc + C.ncx - 1; rb[1] = rowc + C.ncx; nr = lft ? 2 : 1;
           sxr[1] = L;
         } else if (cx == C.ncx - 1) {
-          ra[0] = rowc + cx - 1; rb[0] = rowc + C.ncx; ra[1] = rowc; rb[1] = rowc + 1; nr = 2;
+          ra[0] = rowc + cx - (lft ? 1 : 0); rb[0] = rowc + C.ncx;
+          ra[1] = rowc; rb[1] = rowc + 1; nr = rgt ? 2 : 1;
           sxr[1] = -L;
         } else {
-          ra[0] = rowc + cx - 1; rb[0] = rowc + cx + 2;
+          ra[0] = rowc + cx - (lft ? 1 : 0); rb[0] = rowc + cx + (rgt ? 2 : 1);
         }
         for (int d = 0; d < nr; d++) {
           const int q1 = C.cstart[rb[d]];
           const double sxL = sxr[d];
-          // four candidates' indices loaded ahead of their tests
-          for (int q = C.cstart[ra[d]]; q < q1; q += 4) {
-            int js[4];
+          // kSearchChunk candidates' indices loaded ahead of their tests
+          for (int q = C.cstart[ra[d]]; q < q1; q += kSearchChunk) {
+            int js[kSearchChunk];
 #pragma unroll
-            for (int u = 0; u < 4; u++) js[u] = q + u < q1 ? A.sorted[off + q + u] : i;
+            for (int u = 0; u < kSearchChunk; u++)
+              js[u] = q + u < q1 ? (ident ? q + u : A.sorted[off + q + u]) : i;
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
+            for (int u = 0; u < kSearchChunk; u++) {
               const int j = js[u];
               if (j == i) continue;
               double dx = __dsub_rn(xi, P.x(j)), dy = __dsub_rn(yi, P.y(j)),
@@ -1591,6 +1637,7 @@ struct clmd_ensemble {
   int cl_max_clusters[kClasses] = {};  // co-resident clusters per launch (0: size unusable)
   int cl_region0[kClasses] = {};       // first cell-count region of each cluster class
   bool use_clusters = true;
+  bool cell_order = false;  // every replica in cell order (CLMD_ENS_ORDER=cell)
   cudaStream_t cstream[kClasses] = {};
   cudaEvent_t ev0[kClasses] = {}, ev1[kClasses] = {}, evj = nullptr;
   cudaEvent_t evdone[kClasses] = {};  // join of each class stream
@@ -1751,6 +1798,8 @@ extern "C" int clmd_ens_create(const clmd_ens_config* cfg, clmd_ensemble** out) 
     // CTA each (class 3) instead of on a thread-block cluster
     const char* k = getenv("CLMD_ENS_CLUSTERS");
     E->use_clusters = !(k && k[0] == '0');
+    const char* o = getenv("CLMD_ENS_ORDER");
+    E->cell_order = o && strcmp(o, "cell") == 0;
     // CLMD_ENS_CLASSES="a,b,c": upper atom counts of the first three size
     // classes (ascending), for tuning the split
     const char* cs = getenv("CLMD_ENS_CLASSES");
@@ -1811,6 +1860,12 @@ extern "C" int clmd_ens_create(const clmd_ens_config* cfg, clmd_ensemble** out) 
   A.ftcsi = cfg->ftcsi;
   A.lstride = E->cfg.list_stride;
   A.integrator = cfg->integrator;
+  {
+    // CLMD_ENS_REORDER_EVERY=k: renew the length order at every k-th rebuild
+    // (default 3: measured best of 1, 2 and 3 on the batched workload)
+    const char* r = getenv("CLMD_ENS_REORDER_EVERY");
+    A.reorder_every = (r && atoi(r) > 0) ? atoi(r) : 3;
+  }
   E->used.assign(R, 0);
   E->slot_off.assign(R, -1);
   E->free_list.push_back({0, P});
@@ -1952,7 +2007,9 @@ extern "C" int clmd_ens_add(clmd_ensemble* E, const clmd_replica_spec* sp, const
   // the cell grid never needs more than box / rc cells per dimension (the
   // list radius stays above rc): small boxes keep their shared memory small
   R.ncmax = std::max(1, std::min(cells_for(E->smem_cap, N, &fits), (int)(sp->box / E->cfg.rc)));
-  R.reorder = fits ? 2 : 1;  // (rows of similar length per warp; large: gathers near)
+  // (rows of similar length per warp; large: gathers near).
+  // CLMD_ENS_ORDER=cell: cell order for every replica
+  R.reorder = (fits && !E->cell_order) ? 2 : 1;
   std::vector<int> iota(N);
   for (int i = 0; i < N; i++) iota[i] = (int)off + i;
   ECK(cudaMemcpyAsync(A.orig + off, iota.data(), 4 * (size_t)N, cudaMemcpyHostToDevice, st));
