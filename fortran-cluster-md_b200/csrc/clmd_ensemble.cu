@@ -498,13 +498,19 @@ __device__ void length_order(const Rep& R, Cta& C, const Args& A) {
   int* cnt = lsort;                   // [W][kLenBuckets]
   int* base = cnt + W * kLenBuckets;  // [kLenBuckets]
   // bucket sizes -> bucket starts
-  int mine[kLenBuckets] = {};
-  for (int i = tid; i < N; i += NT) mine[len_bucket(A.rlen[off + i])]++;
+  // bucket sizes per warp by ballots (lane b keeps bucket b's count; no
+  // per-thread array, which would live in local memory)
+  int mine = 0;
+  for (int i0 = 0; i0 < N; i0 += NT) {  // uniform: every thread takes every tile
+    const int i = i0 + tid;
+    const int key = i < N ? len_bucket(A.rlen[off + i]) : -1;
 #pragma unroll
-  for (int b = 0; b < kLenBuckets; b++) {
-    const int t = __reduce_add_sync(0xffffffffu, mine[b]);
-    if (lane == 0) cnt[w * kLenBuckets + b] = t;
+    for (int b = 0; b < kLenBuckets; b++) {
+      const int c = __popc(__ballot_sync(0xffffffffu, key == b));
+      if (lane == b) mine += c;
+    }
   }
+  if (lane < kLenBuckets) cnt[w * kLenBuckets + lane] = mine;
   __syncthreads();
   if (tid == 0) {
     int acc = 0;
@@ -730,8 +736,6 @@ __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
         // the x-neighbours of a cell row are contiguous in cell order: one
         // candidate range, two where the row wraps (all of it when ncx <= 2)
         const int rowc = (zz * C.ncx + yy) * C.ncx;
-        int ra[2], rb[2], nr = 1;
-        double sxr[2] = {0.0, 0.0};
 #if CLMD_SEARCH_PRUNE
         bool lft = true, rgt = true;
         if (!sel) {
@@ -746,24 +750,31 @@ __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
 #else
         const bool lft = true, rgt = true;
 #endif
+        // the x-neighbours of a cell row are contiguous in cell order: one
+        // candidate range [ca0, cb0), a second [ca1, cb1) with image shift
+        // sx1 where the row wraps (all of the row when ncx <= 2).  Scalars
+        // picked per range, not arrays indexed by it: those would live in
+        // local memory.
+        int ca0, cb0, ca1 = 0, cb1 = 0, nr = 1;
+        double sx1 = 0.0;
         if (sel) {
-          ra[0] = rowc; rb[0] = rowc + C.ncx;
+          ca0 = rowc; cb0 = rowc + C.ncx;
         } else if (cx == 0) {
-          ra[0] = rowc; rb[0] = rowc + (rgt ? 2 : 1);
-          ra[1] = rowc + C.ncx - 1; rb[1] = rowc + C.ncx; nr = lft ? 2 : 1;
-          sxr[1] = L;
+          ca0 = rowc; cb0 = rowc + (rgt ? 2 : 1);
+          ca1 = rowc + C.ncx - 1; cb1 = rowc + C.ncx; nr = lft ? 2 : 1;
+          sx1 = L;
         } else if (cx == C.ncx - 1) {
-          ra[0] = rowc + cx - (lft ? 1 : 0); rb[0] = rowc + C.ncx;
-          ra[1] = rowc; rb[1] = rowc + 1; nr = rgt ? 2 : 1;
-          sxr[1] = -L;
+          ca0 = rowc + cx - (lft ? 1 : 0); cb0 = rowc + C.ncx;
+          ca1 = rowc; cb1 = rowc + 1; nr = rgt ? 2 : 1;
+          sx1 = -L;
         } else {
-          ra[0] = rowc + cx - (lft ? 1 : 0); rb[0] = rowc + cx + (rgt ? 2 : 1);
+          ca0 = rowc + cx - (lft ? 1 : 0); cb0 = rowc + cx + (rgt ? 2 : 1);
         }
         for (int d = 0; d < nr; d++) {
-          const int q1 = C.cstart[rb[d]];
-          const double sxL = sxr[d];
+          const int q1 = C.cstart[d ? cb1 : cb0];
+          const double sxL = d ? sx1 : 0.0;
           // kSearchChunk candidates' indices loaded ahead of their tests
-          for (int q = C.cstart[ra[d]]; q < q1; q += kSearchChunk) {
+          for (int q = C.cstart[d ? ca1 : ca0]; q < q1; q += kSearchChunk) {
             int js[kSearchChunk];
 #pragma unroll
             for (int u = 0; u < kSearchChunk; u++)
@@ -913,7 +924,9 @@ __device__ void forces(Rep& R, Cta& C, const Args& A, const Pos<SM>& P, bool kic
       }
     }
   } else
-  for (int i = gt; i < N; i += GT) {
+  for (int i0 = 0; i0 < N; i0 += GT) {
+    const int i = i0 + gt;
+    if (i >= N) continue;
     const double xi = P.x(i), yi = P.y(i), zi = P.z(i);
     const int len = A.rlen[off + i];
     double ax, ay, az;
