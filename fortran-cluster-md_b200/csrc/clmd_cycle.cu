@@ -206,25 +206,28 @@ __device__ __forceinline__ bool nbt(const Params& P, double rs2, const double4& 
   return r2 <= rs2;
 }
 
-__device__ __forceinline__ int xr(const Geo& g, const int* cs, int row, int cx, int* r0,
-                                  int* r1) {
+// the candidate slots of a cell row: [a0, b0) and, where the x-neighbours
+// wrap, [a1, b1) (scalars, not arrays indexed by the range: those would live
+// in local memory)
+__device__ __forceinline__ int xr(const Geo& g, const int* cs, int row, int cx, int& a0,
+                                  int& b0, int& a1, int& b1) {
   int n = g.ncx;
   if (n >= 3) {
     if (cx >= 1 && cx <= n - 2) {
-      r0[0] = cs[row + cx - 1]; r1[0] = cs[row + cx + 2];
+      a0 = cs[row + cx - 1]; b0 = cs[row + cx + 2];
       return 1;
     }
     if (cx == 0) {
-      r0[0] = cs[row]; r1[0] = cs[row + 2];
-      r0[1] = cs[row + n - 1]; r1[1] = cs[row + n];
+      a0 = cs[row]; b0 = cs[row + 2];
+      a1 = cs[row + n - 1]; b1 = cs[row + n];
       return 2;
     }
-    r0[0] = cs[row + n - 2]; r1[0] = cs[row + n];
-    r0[1] = cs[row]; r1[1] = cs[row + 1];
+    a0 = cs[row + n - 2]; b0 = cs[row + n];
+    a1 = cs[row]; b1 = cs[row + 1];
     return 2;
   }
-  r0[0] = cs[row];
-  r1[0] = cs[row + n];
+  a0 = cs[row];
+  b0 = cs[row + n];
   return 1;
 }
 
@@ -246,10 +249,11 @@ __device__ __forceinline__ int scan_cells(const Params& P, const Geo& g, int p, 
       yy += (yy < 0) ? g.ncy : 0;
       yy -= (yy >= g.ncy) ? g.ncy : 0;
       int row = (zz * g.ncy + yy) * g.ncx;
-      int r0[2], r1[2];
-      int nr = xr(g, cs, row, cx, r0, r1);
+      int a0, b0, a1 = 0, b1 = 0;
+      const int nr = xr(g, cs, row, cx, a0, b0, a1, b1);
       for (int r = 0; r < nr; r++) {
-        for (int q = r0[r]; q < r1[r]; q++) {
+        const int qb = r ? b1 : b0;
+        for (int q = r ? a1 : a0; q < qb; q++) {
           if (q == p) continue;
           double4 pq = pos[q];
           int refq = perm[q];
@@ -275,6 +279,10 @@ struct CycleArgs {
   double4* pos1;
   double *vx, *vy, *vz, *ax, *ay, *az;
   double *vxn, *vyn, *vzn;
+  // mixed Nose-Hoover: the accelerations between a step's force pass and its
+  // velocity pass, FP32 (the storage of the FP64 sweeps' iterate vxn..vzn,
+  // which that path does not use)
+  float *afx, *afy, *afz;
   int *perm, *iperm;
   double4* pos_s;
   double *vx_s, *vy_s, *vz_s, *ax_s, *ay_s, *az_s;
@@ -284,21 +292,32 @@ struct CycleArgs {
   double* red;  // 2 x kRedSlots x gridDim partials
 };
 
-// returns false if the grid must stop (error)
+// neighbor-pbc-mav.f:67-71
+__device__ __forceinline__ double4 wrap_box(const Params& P, double4 v) {
+  v.x = fmod(fmod(v.x, P.boxx) + P.boxx, P.boxx);
+  v.y = fmod(fmod(v.y, P.boxy) + P.boxy, P.boxy);
+  v.z = fmod(fmod(v.z, P.boxz) + P.boxz, P.boxz);
+  return v;
+}
+
+// The list rebuild, in place: positions wrapped and, with the velocities and
+// perm, put in cell order (gathered into pos_s, vx_s.., perm_s; the search
+// reads the new order there and copies each slot back as it takes it).
+// Returns false if the grid must stop (error).  acc: carry the accelerations
+// into the new order too; a rebuild inside the step loop runs between the
+// drift (the last reader of a step's accelerations) and the force pass that
+// overwrites them, so there they are not moved
 static __device__ bool rebuild(const Params& P, DevState* st, Blk& B, const CycleArgs& A,
-                        double4* pos, double* sh) {
+                               double4* pos, double* sh, bool acc) {
   const int N = P.N;
   const int G = gridDim.x * blockDim.x;
   const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
   const Geo& g = B.g;
-  // R1: wrap (neighbor-pbc-mav.f:67-71) + histogram
+  // R1: histogram of the wrapped positions (neighbor-pbc-mav.f:67-71; the
+  // gather below stores them wrapped)
   if (t0 == 0) st->list_used = 0ull;
   for (int p = t0; p < N; p += G) {
-    double4 v = pos[p];
-    v.x = fmod(fmod(v.x, P.boxx) + P.boxx, P.boxx);
-    v.y = fmod(fmod(v.y, P.boxy) + P.boxy, P.boxy);
-    v.z = fmod(fmod(v.z, P.boxz) + P.boxz, P.boxz);
-    pos[p] = v;
+    const double4 v = wrap_box(P, pos[p]);
     int cx = min((int)(v.x * g.cfx), g.ncx - 1);
     int cy = min((int)(v.y * g.cfy), g.ncy - 1);
     int cz = min((int)(v.z * g.cfz), g.ncz - 1);
@@ -393,32 +412,24 @@ static __device__ bool rebuild(const Params& P, DevState* st, Blk& B, const Cycl
     }
     for (int q = c0; q < c1; q++) {
       int o = A.cell_atoms[q];
-      A.pos_s[q] = pos[o];
+      A.pos_s[q] = wrap_box(P, pos[o]);
       A.vx_s[q] = A.vx[o];
       A.vy_s[q] = A.vy[o];
       A.vz_s[q] = A.vz[o];
-      A.ax_s[q] = A.ax[o];
-      A.ay_s[q] = A.ay[o];
-      A.az_s[q] = A.az[o];
+      if (acc) {
+        A.ax_s[q] = A.ax[o];
+        A.ay_s[q] = A.ay[o];
+        A.az_s[q] = A.az[o];
+      }
       A.perm_s[q] = A.perm[o];
     }
   }
   if (!gbar(st)) return false;
-  // R6: commit the new order
-  for (int p = t0; p < N; p += G) {
-    pos[p] = A.pos_s[p];
-    A.vx[p] = A.vx_s[p];
-    A.vy[p] = A.vy_s[p];
-    A.vz[p] = A.vz_s[p];
-    A.ax[p] = A.ax_s[p];
-    A.ay[p] = A.ay_s[p];
-    A.az[p] = A.az_s[p];
-    int r = A.perm_s[p];
-    A.perm[p] = r;
-    A.iperm[r] = p;
-  }
-  if (!gbar(st)) return false;
-  // R7: rows (neighbor-pbc-mav.f:73-99), warp-aligned grid-stride
+  // R7: rows (neighbor-pbc-mav.f:73-99), warp-aligned grid-stride, over the
+  // new order in the scratch arrays; each slot is committed (copied back)
+  // by the thread that takes it
+  const double4* npos = A.pos_s;
+  const int* perm = A.perm_s;
   const int lane = threadIdx.x & 31;
   for (int base0 = t0 - lane; base0 < N; base0 += G) {
     int p = base0 + lane;
@@ -427,9 +438,20 @@ static __device__ bool rebuild(const Params& P, DevState* st, Blk& B, const Cycl
     double4 pi = make_double4(0, 0, 0, 0);
     int bq[kRowBufC], bref[kRowBufC];
     if (active) {
-      pi = pos[p];
-      refi = A.perm[p];
-      cnt = scan_cells<false>(P, g, p, refi, pi, pos, A.perm, A.cell_start, bq, bref, nullptr);
+      pi = npos[p];
+      refi = perm[p];
+      pos[p] = pi;
+      A.vx[p] = A.vx_s[p];
+      A.vy[p] = A.vy_s[p];
+      A.vz[p] = A.vz_s[p];
+      if (acc) {
+        A.ax[p] = A.ax_s[p];
+        A.ay[p] = A.ay_s[p];
+        A.az[p] = A.az_s[p];
+      }
+      A.perm[p] = refi;
+      A.iperm[refi] = p;
+      cnt = scan_cells<false>(P, g, p, refi, pi, npos, perm, A.cell_start, bq, bref, nullptr);
     }
     int incl = cnt;
 #pragma unroll
@@ -468,17 +490,17 @@ static __device__ bool rebuild(const Params& P, DevState* st, Blk& B, const Cycl
         lo += bref[a] < refi;
       }
     } else {
-      scan_cells<true>(P, g, p, refi, pi, pos, A.perm, A.cell_start, nullptr, nullptr, row);
+      scan_cells<true>(P, g, p, refi, pi, npos, perm, A.cell_start, nullptr, nullptr, row);
       for (int a = 1; a < cnt; a++) {
-        int kq = row[a], kr = A.perm[kq];
+        int kq = row[a], kr = perm[kq];
         int b = a - 1;
-        while (b >= 0 && A.perm[row[b]] > kr) {
+        while (b >= 0 && perm[row[b]] > kr) {
           row[b + 1] = row[b];
           b--;
         }
         row[b + 1] = kq;
       }
-      for (int a = 0; a < cnt; a++) lo += A.perm[row[a]] < refi;
+      for (int a = 0; a < cnt; a++) lo += perm[row[a]] < refi;
     }
     A.row_start[p] = (int)start;
     A.row_len[p] = cnt;
@@ -718,8 +740,8 @@ __global__ void __launch_bounds__(kPB, CLMD_CYCLE_MINB) k_cycle(Params P, DevSta
   }
   __syncthreads();
   int step = st->cur_step;
-  int cur = 0;  // positions of the current step live in pos[cur]
-  double4* posb[2] = {A.pos0, A.pos1};
+  int cur = 0;  // positions of the current step live in pos0 / pos1
+  auto posb = [&](int k) { return k ? A.pos1 : A.pos0; };
   int rb = 0;  // partial-buffer toggle
   auto red = [&]() { return A.red + (size_t)rb * kRedSlots * gridDim.x; };
 
@@ -730,7 +752,7 @@ __global__ void __launch_bounds__(kPB, CLMD_CYCLE_MINB) k_cycle(Params P, DevSta
       prologue(P, B, step);
     }
     __syncthreads();
-    if (!B.stop) rebuild(P, st, B, A, posb[0], sh);
+    if (!B.stop) rebuild(P, st, B, A, posb(0), sh, true);
     goto done;
   }
 
@@ -768,7 +790,7 @@ __global__ void __launch_bounds__(kPB, CLMD_CYCLE_MINB) k_cycle(Params P, DevSta
         double d2 = 0.0, sv = 0.0;
         const double psi = B.q.psi;
         const double dt2 = dt * dt / 2, dth = dt / 2;
-        double4* pos = posb[cur];
+        double4* pos = posb(cur);
         for (int p = t0; p < N; p += G) {
           double vxi = A.vx[p], vyi = A.vy[p], vzi = A.vz[p];
           if (thermo) {
@@ -833,16 +855,20 @@ __global__ void __launch_bounds__(kPB, CLMD_CYCLE_MINB) k_cycle(Params P, DevSta
         rb ^= 1;
         if (B.stop) goto done;
         if (B.rebuild) {
-          if (!rebuild(P, st, B, A, posb[cur], sh)) goto stop_or_timeout;
+          if (!rebuild(P, st, B, A, posb(cur), sh, false)) goto stop_or_timeout;
         }
       }
       // ---- forces (+ kick, + next drift)
       {
-        double4* pos = posb[cur];
-        double4* nxt = posb[cur ^ 1];
+        double4* pos = posb(cur);
+        double4* nxt = posb(cur ^ 1);
         const double bf1 = 2.0 + (double)(int)(B.q.atrskin / P.sig1);
         const double bf2 = bf1 + 0.5;
         const bool fuse = !nh && !thermo && !last;
+        // mixed Nose-Hoover: the velocity pass fuses the next drift unless
+        // this is the launch's last step or velocities are rescaled first
+        const bool keep64 = last || thermo;
+        (void)keep64;
         double esum = 0.0, vir = 0.0, ek = 0.0, d2 = 0.0, dp = 0.0, sv = 0.0;
         const double psi = B.q.psi;
         const double dth = dt / 2, m = P.apmas[0], Q = P.Q;
@@ -856,7 +882,9 @@ __global__ void __launch_bounds__(kPB, CLMD_CYCLE_MINB) k_cycle(Params P, DevSta
           Pair f;
           f.esum = 0.0;
           f.vir = 0.0;
-          warp_forces<MIXED>(P, st, pos, A.list, act ? A.row_start[p] : 0, act ? A.row_len[p] : 0,
+          // lane 0 is active whenever the warp is; only its row start is used
+          warp_forces<MIXED>(P, st, pos, A.list, lane == 0 ? A.row_start[p] : 0,
+                      act ? A.row_len[p] : 0,
                       act ? A.row_lo[p] : 0, pa, bf1, bf2, f.fx, f.fy, f.fz, f.esum, f.vir, W);
           // lanes past N still evaluated pair terms of their warp's atoms
           esum = esum + f.esum;
@@ -866,9 +894,27 @@ __global__ void __launch_bounds__(kPB, CLMD_CYCLE_MINB) k_cycle(Params P, DevSta
           double iatm = 1.0 / P.apmas[sa - 1];
           // int-verlet-mav.f:76-84: a = 0, AccAtom adds fsum/m
           double axi = 0.0 + f.fx * iatm, ayi = 0.0 + f.fy * iatm, azi = 0.0 + f.fz * iatm;
-          A.ax[p] = axi;
-          A.ay[p] = ayi;
-          A.az[p] = azi;
+          if (MIXED && nh) {
+            // FP32 accelerations (the pair terms' precision); FP64 in the
+            // state only where the next reader is an unfused drift
+            const float fx32 = (float)axi, fy32 = (float)ayi, fz32 = (float)azi;
+            axi = fx32;
+            ayi = fy32;
+            azi = fz32;
+            if (keep64) {
+              A.ax[p] = axi;
+              A.ay[p] = ayi;
+              A.az[p] = azi;
+            } else {
+              A.afx[p] = fx32;
+              A.afy[p] = fy32;
+              A.afz[p] = fz32;
+            }
+          } else {
+            A.ax[p] = axi;
+            A.ay[p] = ayi;
+            A.az[p] = azi;
+          }
           if (!nh) {
             // :86-92
             double vxi = A.vx[p] + 0.5 * axi * dt;
@@ -894,12 +940,9 @@ __global__ void __launch_bounds__(kPB, CLMD_CYCLE_MINB) k_cycle(Params P, DevSta
             A.vy[p] = vyi;
             A.vz[p] = vzi;
           } else if (MIXED) {
-            // closed-form solve (clmd_nh_root): W = V + dth a in place of V,
-            // sv = sum W^2
+            // closed-form solve (clmd_nh_root): sv = sum W^2, W = V + dth a
+            // (the velocity pass forms W again from V and a)
             double wx = A.vx[p] + dth * axi, wy = A.vy[p] + dth * ayi, wz = A.vz[p] + dth * azi;
-            A.vx[p] = wx;
-            A.vy[p] = wy;
-            A.vz[p] = wz;
             sv = sv + wx * wx + wy * wy + wz * wz;
           } else {
             // int-verlet-nh-mav.f:94-120: vn = V, sumv2, first sweep's delps
@@ -982,11 +1025,21 @@ __global__ void __launch_bounds__(kPB, CLMD_CYCLE_MINB) k_cycle(Params P, DevSta
           const double c = 1.0 / (1.0 + dth * pn);
           const bool fuse = !thermo && !last;
           double d2 = 0.0, sv = 0.0;
-          double4* pos = posb[cur];
+          double4* pos = posb(cur);
           for (int p = t0; p < N; p += G) {
-            double vxi = A.vx[p] * c, vyi = A.vy[p] * c, vzi = A.vz[p] * c;
+            double axi, ayi, azi;
             if (fuse) {
-              double axi = A.ax[p], ayi = A.ay[p], azi = A.az[p];
+              axi = A.afx[p];
+              ayi = A.afy[p];
+              azi = A.afz[p];
+            } else {
+              axi = A.ax[p];
+              ayi = A.ay[p];
+              azi = A.az[p];
+            }
+            double vxi = (A.vx[p] + dth * axi) * c, vyi = (A.vy[p] + dth * ayi) * c,
+                   vzi = (A.vz[p] + dth * azi) * c;
+            if (fuse) {
               double dx = dt * vxi + dt2 * (axi - pn * vxi);
               double dy = dt * vyi + dt2 * (ayi - pn * vyi);
               double dz = dt * vzi + dt2 * (azi - pn * vzi);
@@ -1149,6 +1202,9 @@ static CycleArgs cycle_args(clmd_system* S) {
   A.vx = S->vx; A.vy = S->vy; A.vz = S->vz;
   A.ax = S->ax; A.ay = S->ay; A.az = S->az;
   A.vxn = S->vxn; A.vyn = S->vyn; A.vzn = S->vzn;
+  A.afx = reinterpret_cast<float*>(S->vxn);
+  A.afy = reinterpret_cast<float*>(S->vyn);
+  A.afz = reinterpret_cast<float*>(S->vzn);
   A.perm = S->perm; A.iperm = S->iperm;
   A.pos_s = S->pos_s;
   A.vx_s = S->vx_s; A.vy_s = S->vy_s; A.vz_s = S->vz_s;
