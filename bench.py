@@ -423,7 +423,10 @@ def engine_arm(args, w):
     torch.cuda.synchronize()
     kms = statistics.mean(x.elapsed_time(y) for x, y in kev)
     peak, peak_kind = measured_peaks()
-    alg = BYTES_PER_ATOM_STEP * n * cyc
+    # mixed Nose-Hoover keeps the accelerations FP32 between its passes
+    per_atom = BYTES_PER_ATOM_STEP_MIXED if w.get("precision") == clmd.PREC_MIXED \
+        else BYTES_PER_ATOM_STEP
+    alg = per_atom * n * cyc
     achieved = alg / (kms / 1e3) / 1e9
     # the committed captures are of the default sizes; DRAM traffic grows
     # with the atoms (both states exceed L2)

@@ -425,7 +425,7 @@ static __device__ bool rebuild(const Params& P, DevState* st, Blk& B, const Cycl
     }
   }
   if (!gbar(st)) return false;
-  // R7: rows (neighbor-pbc-mav.f:73-99), warp-aligned grid-stride, over the
+  // R6: rows (neighbor-pbc-mav.f:73-99), warp-aligned grid-stride, over the
   // new order in the scratch arrays; each slot is committed (copied back)
   // by the thread that takes it
   const double4* npos = A.pos_s;
