@@ -733,8 +733,6 @@ __device__ bool rebuild(Rep& R, Cta& C, const Args& A, const Pos<SM>& P) {
         const double syL = sel ? 0.0 : (yy < 0 ? L : (yy >= C.ncx ? -L : 0.0));
         yy += yy < 0 ? C.ncx : 0;
         yy -= yy >= C.ncx ? C.ncx : 0;
-        // the x-neighbours of a cell row are contiguous in cell order: one
-        // candidate range, two where the row wraps (all of it when ncx <= 2)
         const int rowc = (zz * C.ncx + yy) * C.ncx;
 #if CLMD_SEARCH_PRUNE
         bool lft = true, rgt = true;
