@@ -15,9 +15,13 @@ A bench step is one window: every running replica advances 100 steps
 (analysis + chk_nucleation first).  metric = atom-steps/s.
 
   value   device-resident windows, whole-job atom-steps / max-over-ranks time.
-  e2e     per window every replica's x, v go host->device from pinned memory
-          through the C ABI, the window runs, x, v come back (+ a 16-byte
-          status per replica).
+  e2e     per window every running replica's x, v go host->device from pinned
+          memory and back through the C ABI (clmd_ens_step_io: the window
+          kernel reads a replica's state from the host arrays when it takes
+          the replica and writes it back when it leaves it, so transfers
+          overlap the other replicas' compute; + a 16-byte status per
+          replica).  separate_copies: the same with clmd_ens_upload, step,
+          clmd_ens_download one after the other.
   roofline  the window kernels (k_ens, 4 size classes concurrently), CUDA
           events inside the library; 120 algorithmic bytes per atom-step
           (x, v FP64 and a FP32, read + written) against measured HBM.
@@ -930,20 +934,32 @@ def batched_arm(args):
     dp = [C.cast(b.data_ptr(), C.POINTER(C.c_double)) for b in bufs]
     lib = e.lib
     lib.clmd_ens_download(e.h, *dp)
-    re0 = {k: v.step for k, v in e.results().items()}
-    barrier()
-    t = time.perf_counter()
-    for _ in range(args.steps):
-        lib.clmd_ens_upload(e.h, *dp)
-        e.step(1)
-        lib.clmd_ens_download(e.h, *dp)
-    e2e_s = time.perf_counter() - t
-    barrier()
-    res = e.results()
-    e2e_units = rk.sum(float(sum(slots[k][0] * (res[k].step - re0[k]) for k in slots)))
-    e2e_value = e2e_units / rk.max(e2e_s)
-    h2d = 6 * 8 * total
-    d2h = 6 * 8 * total + 16 * len(slots)
+
+    def e2e_run(streamed):
+        r0 = e.results()
+        barrier()
+        t = time.perf_counter()
+        for _ in range(args.steps):
+            if streamed:
+                # one call: the window kernel reads each running replica's
+                # x, v from the pinned arrays when it takes the replica and
+                # writes them back when it leaves it
+                e.step_io(1, dp)
+            else:
+                lib.clmd_ens_upload(e.h, *dp)
+                e.step(1)
+                lib.clmd_ens_download(e.h, *dp)
+        el = time.perf_counter() - t
+        barrier()
+        r1 = e.results()
+        units = rk.sum(float(sum(slots[k][0] * (r1[k].step - r0[k].step) for k in slots)))
+        running = sum(slots[k][0] for k in slots if r0[k].done == 0 and r0[k].status == 0)
+        return units / rk.max(el), running
+
+    e2e_copies, _ = e2e_run(False)
+    e2e_value, running = e2e_run(True)
+    h2d = 6 * 8 * running
+    d2h = 6 * 8 * running + 16 * len(slots)
 
     line = None
     extra = dict(pcheck=None, rates=[], dropin_value=None)
@@ -983,7 +999,11 @@ def batched_arm(args):
             "dtype": "f32+f64", "data": "synthetic (seeded)",
             "config": batched_config_json(args, total, tuned, world),
             "e2e": {"value": e2e_value, "unit": "atom-steps/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+                    "d2h_bytes_per_step": d2h,
+                    "how": "clmd_ens_step_io per window: the window kernel reads every running "
+                           "replica's x, v from pinned host memory when it takes the replica "
+                           "and writes them back when it leaves it",
+                    "separate_copies": e2e_copies},
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": profiled_traffic("k_ens_batched"),

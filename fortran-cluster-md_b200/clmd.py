@@ -305,6 +305,7 @@ def load(path: str = LIB_PATH):
         "clmd_ens_upload": ([P, d, d, d, d, d, d], C.c_int),
         "clmd_ens_last_ms": ([P, C.POINTER(C.c_float), C.POINTER(C.c_int64)], C.c_int),
         "clmd_ens_download": ([P, d, d, d, d, d, d], C.c_int),
+        "clmd_ens_step_io": ([P, C.c_int32, d, d, d, d, d, d], C.c_int),
         "clmd_ens_free_atoms": ([P], C.c_int64),
         "clmd_ens_launches": ([P], C.c_int64),
         "clmd_ens_pair_terms": ([P, C.POINTER(C.c_int64)], C.c_int),
@@ -657,6 +658,14 @@ class Ensemble:
         st = self.lib.clmd_ens_step(self.h, nwin)
         if st:
             raise ClmdError(st, "clmd_ens_step")
+
+    def step_io(self, nwin, ptrs):
+        """clmd_ens_step_io: upload, nwin windows and download in one call,
+        the copies done by the window kernel.  ptrs: six ctypes double
+        pointers to pinned host arrays in the upload/download layout."""
+        st = self.lib.clmd_ens_step_io(self.h, nwin, *ptrs)
+        if st:
+            raise ClmdError(st, "clmd_ens_step_io")
 
     def step_timed(self, ms):
         """Balanced step: each replica runs as many MD steps as fit in about

@@ -64,7 +64,7 @@ struct Rep {
   int ncmax;  // cell-grid cap, fixed at admission from this replica's size only
   // the atoms' order inside the engine, fixed at admission (orig[] maps each
   // slot to its atom): 1 (positions too large for shared memory) cell order,
-  // 2 (the others) by the rows' lengths; both renewed at every rebuild
+  // 2 (the others) by the rows' lengths; both renewed at every k-th rebuild
   int reorder;
   int nfull;                // full-list entries (pair terms per force pass) of the last rebuild
   long long pterms;         // pair terms evaluated by this replica's force passes
@@ -93,6 +93,13 @@ struct Args {
   // scatter cursors (kNcMax^3 + 2 ints per cluster, indexed by cluster)
   int* cscr;
   long long cscr_stride;
+  // clmd_ens_step_io: the window kernel itself reads each running replica's
+  // x..vz from pinned host memory when it takes the replica and writes them
+  // back when it leaves it (atom order, replica of slot r at hoff[r] of the
+  // concatenation); nullptr: no host I/O
+  const double *hx, *hy, *hz, *hvx, *hvy, *hvz;
+  double *ox, *oy, *oz, *ovx, *ovy, *ovz;
+  const long long* hoff;
 };
 
 __device__ __forceinline__ double wsum(double v) {
@@ -1202,6 +1209,40 @@ __device__ void analysis(Rep& R, Cta& C, const Args& A, const Pos<SM>& P, int st
 // ---------------------------------------------------------------------------
 // one replica, one window
 // ---------------------------------------------------------------------------
+// clmd_ens_step_io: this replica's state between pinned host memory (atom
+// order) and its pool slots (engine order).  parent[] is free at a window's
+// ends and holds the inverse of orig[] (atom -> slot), so that host memory
+// is read and written in coalesced atom order.
+template <int NT, int CS>
+__device__ void host_io(const Rep& R, const Cta& C, const Args& A, bool in) {
+  const int N = R.natom, off = R.off;
+  const int gt = gtid<NT, CS>();
+  constexpr int GT = NT * CS;
+  int* inv = A.parent + off;
+  for (int i = gt; i < N; i += GT) inv[A.orig[off + i] - off] = i;
+  gsync<CS>();
+  const long long h = A.hoff[C.rep];
+  for (int a = gt; a < N; a += GT) {
+    const long long s = off + inv[a];
+    if (in) {
+      A.x[s] = A.hx[h + a];
+      A.y[s] = A.hy[h + a];
+      A.z[s] = A.hz[h + a];
+      A.vx[s] = A.hvx[h + a];
+      A.vy[s] = A.hvy[h + a];
+      A.vz[s] = A.hvz[h + a];
+    } else {
+      A.ox[h + a] = A.x[s];
+      A.oy[h + a] = A.y[s];
+      A.oz[h + a] = A.z[s];
+      A.ovx[h + a] = A.vx[s];
+      A.ovy[h + a] = A.vy[s];
+      A.ovz[h + a] = A.vz[s];
+    }
+  }
+  gsync<CS>();
+}
+
 template <int NT, bool SM, bool MIXED, int CS>
 __device__ void run_window(Rep& R, Cta& C, const Args& A) {
   const int tid = threadIdx.x;
@@ -1213,6 +1254,7 @@ __device__ void run_window(Rep& R, Cta& C, const Args& A) {
   Pos<SM> P{A, C, off};
   bool vin_n = false;  // uniform: the current velocities are in vxn, not vx
   double vsc = 1.0;    // mixed: the velocities are vn * vsc (clmd_nh_root)
+  if (A.hx) host_io<NT, CS>(R, C, A, true);
   if (SM) {
     for (int i = gt; i < N; i += GT) {
       C.sx[i] = A.x[off + i];
@@ -1494,6 +1536,7 @@ out:
     }
   }
   gsync<CS>();
+  if (A.hx) host_io<NT, CS>(R, C, A, false);
 }
 
 // MINB: CTAs per SM the register budget must allow -- 512 / NT (<= 128
@@ -1634,6 +1677,7 @@ struct clmd_ensemble {
   int* h_iwin = nullptr;   // pinned
   float* h_wtime = nullptr;  // pinned copy of A.wtime
   double* d_stage = nullptr;  // bulk copies in atom order (pool doubles, on first use)
+  long long* d_hoff = nullptr;  // clmd_ens_step_io: each slot's offset in the host arrays
   int4* h_summary = nullptr;  // pinned copy of A.summary
   bool reps_stale = false;    // h_reps older than the device records
   // size classes: each has its own block size, shared-memory budget, stream.
@@ -1892,7 +1936,8 @@ extern "C" int clmd_ens_destroy(clmd_ensemble* E) {
   Args& A = E->A;
   void* ps[] = {A.x, A.y, A.z, A.vx, A.vy, A.vz, A.vxn, A.vyn, A.vzn, A.a, A.list, A.rlen,
                 A.sorted, A.cellid, A.parent, A.cs, A.cl, A.orig, A.reps, A.fpt, A.summary,
-                E->d_items, E->d_ctr, E->d_iwin, A.wtime, E->d_stage, A.cscr};
+                E->d_items, E->d_ctr, E->d_iwin, A.wtime, E->d_stage, A.cscr,
+                E->d_hoff};
   for (void* p : ps)
     if (p) cudaFree(p);
   if (E->h_reps) cudaFreeHost(E->h_reps);
@@ -2701,6 +2746,59 @@ extern "C" int clmd_ens_download(clmd_ensemble* E, double* x, double* y, double*
       h += q.second;
     }
   }
+  ECK(cudaStreamSynchronize(E->stream));
+  return CLMD_OK;
+}
+
+// the device address of pinned host memory (CLMD_ERR_ARG for anything else)
+static int mapped_host(const void* p, void** d) {
+  cudaPointerAttributes at;
+  if (!p || cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return CLMD_ERR_ARG;
+  }
+  if (at.type != cudaMemoryTypeHost || !at.devicePointer) return CLMD_ERR_ARG;
+  *d = at.devicePointer;
+  return CLMD_OK;
+}
+
+extern "C" int clmd_ens_step_io(clmd_ensemble* E, int32_t nwin, double* x, double* y, double* z,
+                                double* vx, double* vy, double* vz) {
+  if (!E || nwin < 1) return CLMD_ERR_ARG;
+  std::lock_guard<std::mutex> lock(E->mu);
+  double* h[6] = {x, y, z, vx, vy, vz};
+  void* d[6];
+  for (int k = 0; k < 6; k++)
+    if (mapped_host(h[k], &d[k])) return CLMD_ERR_ARG;
+  const int R = E->cfg.max_replicas;
+  if (!E->d_hoff) ECK(cudaMalloc(&E->d_hoff, sizeof(long long) * R));
+  // the layout of clmd_ens_upload: occupied slots concatenated in slot order
+  std::vector<long long> hoff(R, 0);
+  long long pos = 0;
+  for (int s = 0; s < R; s++)
+    if (E->used[s]) {
+      hoff[s] = pos;
+      pos += E->h_reps[s].natom;
+    }
+  ECK(cudaMemcpyAsync(E->d_hoff, hoff.data(), sizeof(long long) * R, cudaMemcpyHostToDevice,
+                      E->stream));
+  Args& A = E->A;
+  A.hx = A.ox = (double*)d[0];
+  A.hy = A.oy = (double*)d[1];
+  A.hz = A.oz = (double*)d[2];
+  A.hvx = A.ovx = (double*)d[3];
+  A.hvy = A.ovy = (double*)d[4];
+  A.hvz = A.ovz = (double*)d[5];
+  A.hoff = E->d_hoff;
+  // direct launches: a graph would keep these host addresses
+  const bool graphs = E->use_graphs;
+  E->use_graphs = false;
+  int st = launch_all(E, nwin, E->cls_threads);
+  E->use_graphs = graphs;
+  A.hx = A.hy = A.hz = A.hvx = A.hvy = A.hvz = nullptr;
+  A.ox = A.oy = A.oz = A.ovx = A.ovy = A.ovz = nullptr;
+  A.hoff = nullptr;
+  if (st) return st;
   ECK(cudaStreamSynchronize(E->stream));
   return CLMD_OK;
 }

@@ -332,6 +332,16 @@ int clmd_ens_upload(clmd_ensemble* e, const double* x, const double* y, const do
                     const double* vx, const double* vy, const double* vz);
 int clmd_ens_download(clmd_ensemble* e, double* x, double* y, double* z, double* vx,
                       double* vy, double* vz);
+/* clmd_ens_upload + clmd_ens_step(nwin) + clmd_ens_download in one call, with
+ * the copies done by the window kernel itself: each running replica's x..vz
+ * are read from these host arrays when a CTA takes the replica and written
+ * back when it leaves it, so the transfers of one replica overlap the
+ * compute of the others.  The arrays use the upload/download layout and must
+ * be pinned host memory (cudaMallocHost / cudaHostAlloc / cudaHostRegister:
+ * anything else returns CLMD_ERR_ARG); finished replicas' parts are neither
+ * read nor written.  Returns when the windows are done. */
+int clmd_ens_step_io(clmd_ensemble* e, int32_t nwin, double* x, double* y, double* z,
+                     double* vx, double* vy, double* vz);
 /* First step at which the largest cluster reached each size 1..cap (-1 if
  * not yet). */
 int clmd_ens_fpt(clmd_ensemble* e, int32_t slot, int32_t* fpt, int32_t cap);

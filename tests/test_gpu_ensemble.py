@@ -586,3 +586,68 @@ def test_cluster_replica_matches_single_cta_and_mix(gpu, monkeypatch):
         np.testing.assert_allclose(getattr(c, k), getattr(a, k), rtol=0, atol=1e-9 * box)
     np.testing.assert_allclose(c.vx, a.vx, rtol=0, atol=1e-8)
     assert abs(rc.psi - ra.psi) <= 1e-9 * abs(ra.psi) + 1e-14
+
+
+def test_step_io_matches_upload_step_download(gpu):
+    """clmd_ens_step_io (the window kernel reads each replica's x..vz from
+    pinned host memory when it takes the replica and writes them back when
+    it leaves it) against clmd_ens_upload + clmd_ens_step + clmd_ens_download:
+    the same host arrays bit for bit, with a cluster-size replica among small
+    ones, a replica finished earlier (its part is not touched) and the host
+    arrays changed between calls (the kernel reads them)."""
+    import ctypes as C
+    import torch
+
+    sizes = [400, 1800, 3500, 700, 12000, 2500]
+
+    def make():
+        e = clmd.Ensemble(clmd.ens_config(sum(sizes) + 5000, 16, ftcsi=25))
+        slots = []
+        for k, n in enumerate(sizes):
+            box, arrs = replica_inputs(n, 0.03, 0.75, 300 + k)
+            slots.append(e.add(n, box, 0.75, *arrs, csover=10**6,
+                               budget=25 if k == 3 else 0))
+        e.step(2)  # replica 3 spends its budget: finished
+        return e, slots
+
+    total = sum(sizes)
+    bufs = []
+    for _ in range(2):
+        bufs.append([torch.empty(total, dtype=torch.float64).pin_memory() for _ in range(6)])
+    ptr = [[C.cast(t.data_ptr(), C.POINTER(C.c_double)) for t in b] for b in bufs]
+    e1, s1 = make()
+    e2, s2 = make()
+    assert e1.results()[s1[3]].done == 2
+    for e, p in ((e1, ptr[0]), (e2, ptr[1])):
+        assert e.lib.clmd_ens_download(e.h, *p) == 0
+    for a, b in zip(*bufs):
+        assert torch.equal(a, b)
+    # the host copies are what the kernel starts from: change them alike
+    for b in bufs:
+        b[3][100:200] *= 1.01
+        b[0][sizes[0] + 17] += 0.05
+    for t in bufs[1]:
+        t[sum(sizes[:3]):sum(sizes[:4])] = -1.0  # the finished replica's part
+    for _ in range(2):
+        assert e1.lib.clmd_ens_upload(e1.h, *ptr[0]) == 0
+        e1.step(2)
+        assert e1.lib.clmd_ens_download(e1.h, *ptr[0]) == 0
+        e2.step_io(2, ptr[1])
+    lo, hi = sum(sizes[:3]), sum(sizes[:4])
+    for a, b in zip(*bufs):
+        assert torch.equal(a[:lo], b[:lo]) and torch.equal(a[hi:], b[hi:])
+        assert torch.all(b[lo:hi] == -1.0)
+    r1, r2 = e1.results(), e2.results()
+    for k in range(len(sizes)):
+        assert r1[s1[k]].step == r2[s2[k]].step and r1[s1[k]].psi == r2[s2[k]].psi
+        st1, cl1 = e1.state(s1[k])
+        st2, cl2 = e2.state(s2[k])
+        for name in ("x", "y", "z", "vx", "vy", "vz"):
+            assert np.array_equal(getattr(st1, name), getattr(st2, name)), (k, name)
+        assert np.array_equal(cl1, cl2)
+    # memory the device cannot address is refused
+    plain = [np.zeros(total) for _ in range(6)]
+    with pytest.raises(clmd.ClmdError):
+        e2.step_io(1, [a.ctypes.data_as(C.POINTER(C.c_double)) for a in plain])
+    e1.close()
+    e2.close()
