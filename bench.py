@@ -1195,7 +1195,7 @@ def big_replica_ms_per_step(n=50000, rho=0.03, temp=0.75, windows=3):
         out.append(el * 1e3 / (e.results()[slot].step - s0))
         e.close()
     cs = 2
-    while cs < 16 and cs * 3072 < n:
+    while cs < 16 and cs * 6144 < n:
         cs *= 2
     return out[0], out[1], cs
 

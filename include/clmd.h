@@ -276,7 +276,7 @@ int clmd_ens_add(clmd_ensemble* e, const clmd_replica_spec* spec, const double* 
  * persistent launch per size class, the classes concurrently); replicas stop
  * when done.  A replica runs on one CTA, or -- when its positions do not fit
  * in one SM's shared memory (about 9,000 atoms and more) -- on a
- * thread-block cluster of 2, 4, 8 or 16 CTAs (about 3,072 atoms per CTA or
+ * thread-block cluster of 2, 4, 8 or 16 CTAs (about 6,144 atoms per CTA or
  * more) that splits its atoms and meets at cluster barriers
  * (CLMD_ENS_CLUSTERS=0 in the environment at creation: one CTA each).  The
  * launch sequence is captured once into a CUDA graph and replayed while the

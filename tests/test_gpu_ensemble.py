@@ -509,7 +509,7 @@ def test_failed_replica_is_isolated(gpu):
         assert np.array_equal(xa.x, xb.x) and np.array_equal(xa.vz, xb.vz)
 
 
-CLUSTER_SIZES = [(12000, 0.03), (26000, 0.02), (52000, 0.04)]  # 4, 16 and 16 CTAs
+CLUSTER_SIZES = [(12000, 0.03), (26000, 0.02), (52000, 0.04)]  # 2, 8 and 16 CTAs
 
 
 @pytest.mark.parametrize("precision,tol", [(clmd.PREC_MIXED, 1e-5), (clmd.PREC_FP64, 1e-12)])
