@@ -37,7 +37,10 @@ A bench step is one window: every running replica advances 100 steps
   served  configs[4] on the same GPU: a bounded Poisson window at 200
           requests/s served with continuous batching; p50/p99 request
           latency (censored requests at their lower bound), time to
-          nucleation (wall and step), aggregate atom-steps/s.
+          nucleation (wall and step), aggregate atom-steps/s.  Under
+          "drained": a 1 s window of the same arrivals served until every
+          request finished (90 s cap), so its percentiles are uncensored
+          when everything finished.
   cpu_baseline  the serial C restatement of the reference (the oracle) on
           one pinned core, on 16 replicas at the midpoints of 16 size strata,
           3 timed 100-step windows: the rate of exactly that timed work.
@@ -1216,6 +1219,17 @@ def served_leg(args, rk):
          "value": units / wall, "unit": "atom-steps/s", "gpu_launches": int(launches),
          "pool_atoms": pool, "max_resident_replicas": args.served_slots, "clocks": clk}
     d.update(served_summary(out, st, len(reqs), args.served_cap))
+    if args.served_drain_arrival > 0:
+        # a shorter trace served until every request finished (or the cap):
+        # percentiles without censored requests, as far as the cap allows
+        out2, st2, _, _, _, reqs2 = run_served(args, rk, args.served_drain_arrival,
+                                               args.served_drain_cap, args.served_slots)
+        dd = {"workload": f"served-poisson-{SERVED['rate']:.0f}req/s-for-"
+                          f"{args.served_drain_arrival}s, served until drained "
+                          f"(cap {args.served_drain_cap}s), same distributions",
+              "value": rk.sum(st2.atom_steps) / rk.max(st2.wall), "unit": "atom-steps/s"}
+        dd.update(served_summary(out2, st2, len(reqs2), args.served_drain_cap))
+        d["drained"] = dd
     if rk.rank == 0:
         cl_ms, cta_ms, cs = big_replica_ms_per_step()
         d["one_replica_50000_atoms"] = {
@@ -1312,6 +1326,11 @@ def main():
                          "precision check or served leg; for profiler runs)")
     ap.add_argument("--served-arrival", type=float, default=10.0,
                     help="batched: Poisson arrival window of the served leg (s)")
+    ap.add_argument("--served-drain-arrival", type=float, default=1.0,
+                    help="served leg: seconds of arrivals of a second trace served until "
+                         "drained (0: skip)")
+    ap.add_argument("--served-drain-cap", type=float, default=90.0,
+                    help="served leg: wall-clock cap of the drained trace")
     ap.add_argument("--served-cap", type=float, default=30.0,
                     help="batched: wall-clock cap of the served leg (s)")
     ap.add_argument("--served-slots", type=int, default=16384,
