@@ -34,7 +34,7 @@ A bench step is one window: every running replica advances 100 steps
           (1e-13 apart) for 1e4 steps: per-replica energy drift, mixed - FP64
           against the twin's spread, the drift of the energy the truncated
           force conserves, the cluster-size distribution.
-  served  configs[4] on the same GPU: a bounded Poisson window at 200
+  served  the served workload on the same GPU: a bounded Poisson window at 200
           requests/s served with continuous batching; p50/p99 request
           latency (censored requests at their lower bound), time to
           nucleation (wall and step), aggregate atom-steps/s.  Under
@@ -986,7 +986,7 @@ def batched_arm(args):
                      for k in slots)
         dropin_value = sum(slots[k][0] * 100 for k in slots) / t_drop
         extra = dict(pcheck=pcheck, rates=rates, dropin_value=dropin_value)
-    # ---- served leg: a bounded Poisson window on this GPU
+    # ---- served leg: a bounded Poisson window of requests on this GPU
     served = None if (args.no_served or args.no_extras) else served_leg(args, rk)
     if rank == 0:
         cpu = None
@@ -1204,7 +1204,7 @@ def big_replica_ms_per_step(n=50000, rho=0.03, temp=0.75, windows=3):
 
 
 def served_leg(args, rk):
-    """configs[4] inside the default bench: a bounded Poisson window at 200
+    """The served workload inside the default bench: a bounded Poisson window at 200
     requests/s (N log-uniform in [100, 50000], rho* and T* uniform, budgets
     log-uniform in [1e4, 1e6], threshold largest cluster > 100), served with
     continuous batching on this GPU until every request finished or the cap
